@@ -1,0 +1,383 @@
+"""Benchmark of the RK4 time-stepping path on B200.
+
+Workload (the configuration the headline metric is quoted on): FD scheme
+(central FD4 + KO3), periodic z in [-3000, 3000] with nz = 32768, nvz = 256,
+mu = 1, omega = 1e-3, normal ordering, theta = 1e-6 deg, CFL 0.4, FP64,
+seeded synthetic initial condition (sigma_nu 0.6, sigma_nubar 0.5,
+alpha 0.9, +-1e-6 ex).  A "step" is one RK4 step over the whole grid; the
+metric is cell-updates/s = nz * nvz * steps / time.
+
+  value  device-resident: K steps timed with CUDA events on the stream the
+         kernels run on (per stage, so the dominant kernel's duration is
+         measured in the same region); the state (537 MB per buffer) is far
+         larger than L2, so no flush is needed between steps.
+  e2e    through the public API with host buffers: pinned host state ->
+         upload -> K steps with on-device analysis every 40 steps (the
+         reference driver's ANAL_EVERY for this run) -> download.
+  cpu_baseline / --impl reference: the reference's own CPU build
+         (oracle/_ref, compiled from its sources with its --mcore flags)
+         on a z-subset of the same grid, all host threads.
+
+Multi-GPU (torchrun): every rank evolves its own instance (different seed),
+no data-path collective; value = all ranks' cell-updates / max-over-ranks
+time ("weak" scaling).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "cell-updates/s (nz*nvz*RK4 steps), FP64"
+UNIT = "cell-updates/s"
+WORKLOAD = dict(nz=32768, nvz=256, gz=2, z0=-3000.0, z1=3000.0, v0=-1.0, v1=1.0, cfl=0.4,
+                pmo=1.0, omega=1e-3, theta_deg=1e-6, mu=1.0, scheme="fd")
+IC = dict(sig_nu=0.6, sig_nubar=0.5, alpha=0.9, amp=1e-6)
+SEED = 20240601
+ANAL_EVERY = 40  # manage.py: N_ITER = 4000 steps, n_analyze = 100
+PASSES = (3, 5, 5, 3)  # state passes (x 64 B) per cell of stages 1..4
+FALLBACK_HBM_GBS = 6650.0
+
+
+def peak_hbm():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        d = json.load(open(p))
+        return float(d["hbm_gbs"]), "measured (MEASURED_PEAKS.json hbm_gbs)"
+    except Exception:
+        return FALLBACK_HBM_GBS, "fallback"
+
+
+def traffic_from_profile():
+    """Per-launch DRAM bytes of the stage-2 FD kernel from the committed ncu
+    summary (scaled to the full grid there), or None."""
+    p = os.path.join(ROOT, "profiles", "traffic.json")
+    try:
+        return json.load(open(p))
+    except Exception:
+        return None
+
+
+# ---------------------------------------------------------------------------
+class ClockSampler:
+    """nvidia-smi sampling of SM clocks and throttle reasons during a region."""
+    FIELDS = ("clocks.sm", "clocks.max.sm", "power.draw", "clocks_event_reasons.hw_slowdown",
+              "clocks_event_reasons.hw_thermal_slowdown",
+              "clocks_event_reasons.sw_thermal_slowdown", "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index: int):
+        self.dev = device_index
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.dev), "--query-gpu=" + ",".join(self.FIELDS),
+                 "--format=csv,noheader,nounits", "-lms", "100"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+        time.sleep(0.25)
+        return self
+
+    def _read(self):
+        for ln in self.proc.stdout:
+            self.lines.append(ln.strip())
+
+    def __exit__(self, *exc):
+        if self.proc:
+            time.sleep(0.15)
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], [], set()
+        names = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) != len(self.FIELDS):
+                continue
+            try:
+                sm.append(float(f[0]))
+                mx.append(float(f[1]))
+            except ValueError:
+                continue
+            for n, v in zip(names, f[3:]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(mx),
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ---------------------------------------------------------------------------
+def dist_setup(ngpus: int):
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world != ngpus and world > 1:
+        raise SystemExit(f"--gpus {ngpus} but WORLD_SIZE {world}")
+    return rank, world, local
+
+
+def run_ours(args):
+    import datetime
+
+    import numpy as np
+    import torch
+
+    from cosenu_b200 import NuOsc
+
+    rank, world, local = dist_setup(args.gpus)
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local))
+
+    def barrier():
+        torch.cuda.synchronize()
+        if dist:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    stream = torch.cuda.Stream()
+    torch.cuda.set_stream(stream)
+    sim = NuOsc(device=local, **WORKLOAD)
+    sim.set_stream(stream.cuda_stream)
+    cells = WORKLOAD["nz"] * WORKLOAD["nvz"]
+    sim.init_seeded(SEED + rank, **IC)
+    for _ in range(args.warmup):
+        sim.step_rk4()
+    barrier()
+
+    # ---- device-resident timed region: K steps, events around every stage
+    K = args.steps
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(4 * K + 1)]
+    with ClockSampler(local) as clk:
+        barrier()
+        ev[0].record(stream)
+        for k in range(K):
+            for s in range(4):
+                sim.step_stage(s)
+                ev[4 * k + s + 1].record(stream)
+        torch.cuda.synchronize()
+    barrier()
+    total_ms = ev[0].elapsed_time(ev[-1])
+    stage_ms = [0.0] * 4
+    for k in range(K):
+        for s in range(4):
+            stage_ms[s] += ev[4 * k + s].elapsed_time(ev[4 * k + s + 1])
+    stage_ms = [t / K for t in stage_ms]
+    if dist:
+        t = torch.tensor([total_ms], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        total_ms = float(t.item())
+    value = cells * K * world / (total_ms / 1e3)
+    diag = sim.analyse()
+    if not math.isfinite(diag["M0"]):
+        raise SystemExit("non-finite state after the timed region")
+
+    # ---- end to end through the public API with pinned host buffers
+    host0 = sim.download()
+    pinned = torch.from_numpy(host0).pin_memory()
+    hbuf = pinned.numpy()
+    out_pinned = torch.empty_like(pinned).pin_memory()
+    obuf = out_pinned.numpy()
+    barrier()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    n_anal = 0
+    e0.record(stream)
+    sim.upload(hbuf)
+    sim.mark_state0()
+    done = 0
+    while done < K:
+        n = min(ANAL_EVERY, K - done)
+        sim.evolve(n)
+        done += n
+        if done % ANAL_EVERY == 0:
+            sim.analyse()
+            n_anal += 1
+    from cosenu_b200.nuosc import _ptrs
+    sim._check(sim.lib.cosenu_download(sim.h, _ptrs(obuf), sim.gz))
+    e1.record(stream)
+    torch.cuda.synchronize()
+    e2e_ms = e0.elapsed_time(e1)
+    if dist:
+        t = torch.tensor([e2e_ms], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_ms = float(t.item())
+    e2e = cells * K * world / (e2e_ms / 1e3)
+    state_bytes = 8 * WORKLOAD["nvz"] * (WORKLOAD["nz"] + 2 * WORKLOAD["gz"]) * 8
+    h2d = state_bytes / K
+    d2h = (state_bytes + n_anal * 13 * 8) / K
+
+    tz, tv = sim.tile()
+    result = None
+    if rank == 0:
+        peak, peak_src = peak_hbm()
+        dom = 1  # stage 2 (5 passes), same kernel shape as stage 3
+        algo_bytes = PASSES[dom] * 64 * cells
+        achieved = algo_bytes / (stage_ms[dom] / 1e3) / 1e9
+        tr = traffic_from_profile()
+        traffic = tr.get("fd_stage2_bytes_per_launch") if tr else None
+        cpu = cpu_baseline(args) if (world == 1 and not args.no_cpu_baseline) else None
+        result = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": K,
+            "warmup": args.warmup, "ms_per_step": total_ms / K, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": "FD (central FD4 + KO3) RK4, nz 32768 x nvz 256, periodic, "
+                                   "mu 1, omega 1e-3, theta 1e-6 deg",
+                       "nz": WORKLOAD["nz"], "nvz": WORKLOAD["nvz"], "scheme": "FD",
+                       "precision": "FP64", "tile": [tz, tv],
+                       "l2": "inputs larger than L2 (537 MB per state buffer)",
+                       "instances_per_gpu": 1},
+            "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": h2d,
+                    "d2h_bytes_per_step": d2h,
+                    "note": f"upload once, {K} steps, analysis every {ANAL_EVERY} steps, "
+                            "download once"},
+            "gpu_launches": 4 * K,
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "traffic": traffic,
+                         "kernel": "rk4_stage_kernel<FD, stage 2> (5 state passes)",
+                         "algorithmic_bytes_per_launch": algo_bytes,
+                         "avg_launch_ms": stage_ms[dom], "peak_source": peak_src},
+            "stage_ms": stage_ms,
+            "step_hbm_frac": (1024 * cells / (total_ms / K / 1e3) / 1e9) / peak,
+            "clocks": clk.summary(),
+            "cpu_baseline": cpu,
+        }
+        print(json.dumps(result), flush=True)
+    sim.close()
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    return result
+
+
+# ---------------------------------------------------------------------------
+def _ref_exe():
+    from oracle.build import ref_binary
+    exe = ref_binary("fd")
+    if not os.path.exists(exe):
+        raise FileNotFoundError(exe)
+    return exe
+
+
+def _ref_run(nz_sample: int, nsteps: int, threads: int):
+    """Reference FD binary on a z-subset of the workload grid (same dz, nvz,
+    physics), through its --ff path; returns the loop seconds (time.txt)."""
+    from oracle.oracle import Case, Oracle, run_reference
+    w = WORKLOAD
+    dz = (w["z1"] - w["z0"]) / w["nz"]
+    case = Case(nz=nz_sample, nvz=w["nvz"], gz=w["gz"], z0=-0.5 * nz_sample * dz,
+                z1=0.5 * nz_sample * dz, cfl=w["cfl"], pmo=w["pmo"], omega=w["omega"],
+                theta_deg=w["theta_deg"], mu=w["mu"], scheme="fd")
+    o = Oracle()
+    G, bG, st0 = o.init_seeded(case, seed=SEED, **IC)
+    n_iter = max(nsteps + 1, 10)
+    r = run_reference(case, G, bG, st0, n_iter=n_iter, anal_every=n_iter + 1, n_dump_rho=0,
+                      nthreads=threads)
+    return r["loop_seconds"], n_iter - 1
+
+
+def cpu_baseline(args, budget_s: float = 20.0):
+    """~10-30 s of the reference's own CPU path on this host's cores."""
+    try:
+        _ref_exe()
+    except FileNotFoundError:
+        return None
+    threads = os.cpu_count() or 1
+    nvz = WORKLOAD["nvz"]
+    t, n = _ref_run(64, 9, threads)  # calibration
+    per_cell_step = t / (64 * nvz * n)
+    nz = 64
+    while nz * 2 <= WORKLOAD["nz"] and per_cell_step * nz * 2 * nvz * 9 <= budget_s:
+        nz *= 2
+    t, n = _ref_run(nz, 9, threads)
+    return {"value": nz * nvz * n / t, "unit": UNIT, "cores": threads, "kind": "reference",
+            "sample": f"reference FD build (g++ -O3 -fopenmp, OMP_NUM_THREADS={threads}), "
+                      f"{n} RK4 steps on a z-subset nz={nz} of the workload grid "
+                      f"(same dz, nvz={nvz}, physics), loop time from its time.txt"}
+
+
+def run_reference_arm(args):
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    if rank != 0:
+        return
+    try:
+        _ref_exe()
+    except FileNotFoundError as e:
+        print(json.dumps({"impl": "reference", "unavailable": f"reference build missing: {e}"}))
+        return
+    threads = os.cpu_count() or 1
+    nvz = WORKLOAD["nvz"]
+    # size the z-subset so that warm-up + K steps take about two minutes
+    t, n = _ref_run(64, 9, threads)
+    per_cell_step = t / (64 * nvz * n)
+    K, W = max(args.steps, 9), args.warmup
+    nz = 64
+    while nz * 2 <= WORKLOAD["nz"] and per_cell_step * nz * 2 * nvz * (K + W) <= 120.0:
+        nz *= 2
+    if W > 0:
+        _ref_run(nz, max(W, 9), threads)
+    t, n = _ref_run(nz, K, threads)
+    value = nz * nvz * n / t
+    sample = (f"reference FD build (g++ -O3 -fopenmp, OMP_NUM_THREADS={threads}), {n} RK4 "
+              f"steps on a z-subset nz={nz} of the workload grid (same dz, nvz={nvz}, physics); "
+              "loop time from its time.txt")
+    print(json.dumps({
+        "metric": METRIC, "value": value, "unit": UNIT, "impl": "reference", "n_gpus": world,
+        "steps": n, "warmup": W, "ms_per_step": t / n * 1e3, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": "FD (central FD4 + KO3) RK4, nz 32768 x nvz 256, periodic, "
+                               "mu 1, omega 1e-3, theta 1e-6 deg", "sample_nz": nz},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "reference",
+                         "sample": sample},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=1000)
+    ap.add_argument("--warmup", type=int, default=10)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--nz", type=int, default=WORKLOAD["nz"],
+                    help="smaller z extent at the same dz (profiling cases only; the headline "
+                         "workload is nz = 32768)")
+    args = ap.parse_args()
+    if args.nz != WORKLOAD["nz"]:
+        dz = (WORKLOAD["z1"] - WORKLOAD["z0"]) / WORKLOAD["nz"]
+        WORKLOAD.update(nz=args.nz, z0=-0.5 * args.nz * dz, z1=0.5 * args.nz * dz)
+    if args.warmup < 3 and args.impl == "ours":
+        args.warmup = 3
+    if args.impl == "reference":
+        run_reference_arm(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

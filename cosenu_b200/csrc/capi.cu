@@ -1,0 +1,724 @@
+// C ABI of the B200 RK4 path (declarations and reference citations in
+// include/cosenu_b200.h).  A context owns the device state of one simulation
+// and replays the four stage kernels of an RK4 step, captured once into CUDA
+// graphs, for as many steps as the driver asks for.
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/cosenu_b200.h"
+#include "common.cuh"
+
+namespace cosenu {
+cudaError_t launch_rk4_stage(const StageArgs &a, int scheme, int stage, int tz, int fp32,
+                             cudaStream_t s);
+cudaError_t launch_ghost_fill(double *buf, long long cs, int ld, int nz, int nvz, int H, int bc,
+                              cudaStream_t s);
+cudaError_t launch_moments(const double *X, double *M, const double *vz, long long cs, int ld,
+                           int nz, int nvz, int tz, int tv, cudaStream_t s);
+int diag_blocks();
+int diag_slots();
+cudaError_t launch_diag(const double *Y, const double *S0, const double *G, const double *bG,
+                        long long cs, int ld, int nz, int nvz, double dz, double dv, double *part,
+                        double *out, cudaStream_t s);
+cudaError_t launch_pee_v(const double *Y, const double *S0, long long cs, int ld, int nz, int nvz,
+                         double *out, cudaStream_t s);
+cudaError_t launch_init_seeded(double *Y, double *G, double *bG, const double *Gv,
+                               const double *bGv, long long cs, int ld, int nz, int nvz,
+                               uint64_t seed, uint32_t instance, double amp, cudaStream_t s);
+cudaError_t launch_init_reference(double *Y, double *G, double *bG, const double *Gv,
+                                  const double *bGv, const double *ez, const double *ez_,
+                                  long long cs, int ld, int nz, int nvz, cudaStream_t s);
+}  // namespace cosenu
+
+using namespace cosenu;
+
+static thread_local std::string g_create_error;
+
+struct cosenu_ctx {
+    cosenu_params p{};
+    int ld = 0, H = 4, tz = 32, tv = 64, nvt = 1;
+    long long cs = 0;
+    double dz = 0, dv = 0, dt = 0, ct = 0, st = 0;
+    int fp32 = 0;
+    cudaStream_t own_stream = nullptr, stream = nullptr;
+    // device memory
+    double *Y = nullptr, *A = nullptr, *S0 = nullptr, *G = nullptr, *bG = nullptr;
+    void *U0 = nullptr, *U1 = nullptr;
+    double *M[3] = {nullptr, nullptr, nullptr};
+    double *vz = nullptr, *rowfac = nullptr, *Hm = nullptr;
+    double *diag_part = nullptr, *diag_out = nullptr, *pee = nullptr, *tmp = nullptr;
+    size_t bytes = 0;
+    // host mirrors
+    std::vector<double> h_vz, h_rowfac, h_Hm, h_Z;
+    double *h_pinned = nullptr;  // small pinned buffer for results
+    // graphs of 1 and GRAPH_CHUNK steps
+    cudaGraphExec_t g1 = nullptr, gN = nullptr;
+    bool use_graphs = true;
+    // status
+    bool have_state = false, have_profile = false, have_state0 = false;
+    int next_stage = 0;
+    long long steps = 0;
+    std::string err;
+};
+
+static const int GRAPH_CHUNK = 16;
+
+#define CK(call)                                                                              \
+    do {                                                                                      \
+        cudaError_t e_ = (call);                                                              \
+        if (e_ != cudaSuccess) {                                                              \
+            ctx->err = std::string(#call) + ": " + cudaGetErrorString(e_);                    \
+            return COSENU_ERR_CUDA;                                                           \
+        }                                                                                     \
+    } while (0)
+
+namespace {
+
+struct DeviceGuard {
+    int prev = -1;
+    explicit DeviceGuard(int dev)
+    {
+        if (cudaGetDevice(&prev) != cudaSuccess) prev = -1;
+        if (prev != dev) cudaSetDevice(dev);
+    }
+    ~DeviceGuard()
+    {
+        int cur = -1;
+        if (prev >= 0 && cudaGetDevice(&cur) == cudaSuccess && cur != prev) cudaSetDevice(prev);
+    }
+};
+
+int fail(cosenu_ctx *ctx, int code, const std::string &msg)
+{
+    if (ctx) ctx->err = msg;
+    return code;
+}
+
+// normalised Gaussian angular profile, src/miscellaneous_funcs.hpp:57-62
+double gprof(double v, double v0, double sigma)
+{
+    double e = (v - v0) * (v - v0) / (2.0 * sigma * sigma);
+    double N = sigma * sqrt(M_PI / 2.0) *
+               (erf((1.0 + v0) / sigma / sqrt(2.0)) + erf((1.0 - v0) / sigma / sqrt(2.0)));
+    return exp(-e) / N;
+}
+
+int alloc(cosenu_ctx *ctx, void **p, size_t n)
+{
+    cudaError_t e = cudaMalloc(p, n);
+    if (e != cudaSuccess) {
+        ctx->err = "cudaMalloc(" + std::to_string(n) + " B): " + cudaGetErrorString(e);
+        return e == cudaErrorMemoryAllocation ? COSENU_ERR_NOMEM : COSENU_ERR_CUDA;
+    }
+    ctx->bytes += n;
+    return COSENU_OK;
+}
+
+void choose_tile(cosenu_ctx *ctx)
+{
+    const cosenu_params &p = ctx->p;
+    int tz = p.tile_z;
+    if (tz == 0) tz = (p.nz % 32 == 0) ? 32 : (p.nz % 16 == 0 ? 16 : 8);
+    int rp = NTHREADS / tz;
+    int tv = p.tile_v;
+    if (tv == 0) {
+        tv = std::min(p.nvz, 64);
+        // enough blocks to fill 148 SMs several times over
+        while (tv > rp && (long long)(p.nz / tz) * ((p.nvz + tv - 1) / tv) < 8 * 148) tv /= 2;
+        if (tv < 1) tv = 1;
+    }
+    ctx->tz = tz;
+    ctx->tv = tv;
+    ctx->nvt = (p.nvz + tv - 1) / tv;
+}
+
+StageArgs stage_args(const cosenu_ctx *ctx, int stage)
+{
+    StageArgs a{};
+    a.vz = ctx->vz;
+    a.rowfac = ctx->rowfac;
+    a.Hm = ctx->Hm;
+    a.cs = ctx->cs;
+    a.nz = ctx->p.nz;
+    a.nvz = ctx->p.nvz;
+    a.ld = ctx->ld;
+    a.tv = ctx->tv;
+    a.nvt = ctx->nvt;
+    a.H = ctx->H;
+    a.bc = ctx->p.bc;
+    a.flags = (int)ctx->p.flags;
+    a.fd_advec = ctx->p.fd_advec;
+    a.ko_order = ctx->p.ko_order;
+    a.dt = ctx->dt;
+    a.dv = ctx->dv;
+    a.mu = ctx->p.mu;
+    a.ct = ctx->ct;
+    a.st = ctx->st;
+    a.pmo = ctx->p.pmo;
+    const double ko = 1.0e-1;  // src/nuosc.hpp:60
+    a.ko_eps = ctx->p.ko_order == 5 ? -ko / ctx->dz / 64.0 : -ko / ctx->dz / 16.0;
+    a.Y = ctx->Y;
+    a.A = ctx->A;
+    switch (stage) {
+    case 1: a.X = ctx->Y; a.U = ctx->U0; a.Min = ctx->M[2]; a.Mout = ctx->M[0]; break;
+    case 2: a.X = ctx->U0; a.U = ctx->U1; a.Min = ctx->M[0]; a.Mout = ctx->M[1]; break;
+    case 3: a.X = ctx->U1; a.U = ctx->U0; a.Min = ctx->M[1]; a.Mout = ctx->M[0]; break;
+    case 4: a.X = ctx->U0; a.U = ctx->Y; a.Min = ctx->M[0]; a.Mout = ctx->M[2]; break;
+    }
+    return a;
+}
+
+cudaError_t launch_stage(cosenu_ctx *ctx, int stage, cudaStream_t s)
+{
+    StageArgs a = stage_args(ctx, stage);
+    return launch_rk4_stage(a, ctx->p.scheme, stage, ctx->tz, ctx->fp32, s);
+}
+
+cudaError_t launch_steps(cosenu_ctx *ctx, int n, cudaStream_t s)
+{
+    for (int i = 0; i < n; ++i)
+        for (int st = 1; st <= 4; ++st) {
+            cudaError_t e = launch_stage(ctx, st, s);
+            if (e != cudaSuccess) return e;
+        }
+    return cudaSuccess;
+}
+
+// Captures `n` steps into an executable graph (on a private stream).
+cudaError_t capture(cosenu_ctx *ctx, int n, cudaGraphExec_t *out)
+{
+    cudaStream_t cs;
+    cudaError_t e = cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking);
+    if (e != cudaSuccess) return e;
+    cudaGraph_t g = nullptr;
+    e = cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal);
+    if (e == cudaSuccess) {
+        cudaError_t le = launch_steps(ctx, n, cs);
+        e = cudaStreamEndCapture(cs, &g);
+        if (le != cudaSuccess) e = le;
+    }
+    if (e == cudaSuccess) e = cudaGraphInstantiate(out, g, 0);
+    if (g) cudaGraphDestroy(g);
+    cudaStreamDestroy(cs);
+    return e;
+}
+
+// Refreshes ghosts and input moments of Y after Y changed outside the stages.
+int prepare_state(cosenu_ctx *ctx)
+{
+    CK(launch_ghost_fill(ctx->Y, ctx->cs, ctx->ld, ctx->p.nz, ctx->p.nvz, ctx->H, ctx->p.bc,
+                         ctx->stream));
+    if (ctx->p.flags & COSENU_COLL)
+        CK(launch_moments(ctx->Y, ctx->M[2], ctx->vz, ctx->cs, ctx->ld, ctx->p.nz, ctx->p.nvz,
+                          ctx->tz, ctx->tv, ctx->stream));
+    ctx->have_state = true;
+    ctx->next_stage = 0;
+    return COSENU_OK;
+}
+
+int copy_planes_h2d(cosenu_ctx *ctx, double *dst, const double *const *src, int ncomp, int gz)
+{
+    const int nz = ctx->p.nz, nvz = ctx->p.nvz;
+    for (int c = 0; c < ncomp; ++c) {
+        if (!src[c]) return fail(ctx, COSENU_ERR_ARG, "null component pointer");
+        CK(cudaMemcpy2DAsync(dst + (long long)c * ctx->cs + HP, (size_t)ctx->ld * 8, src[c] + gz,
+                             (size_t)(nz + 2 * gz) * 8, (size_t)nz * 8, nvz,
+                             cudaMemcpyHostToDevice, ctx->stream));
+    }
+    return COSENU_OK;
+}
+
+void drop_graphs(cosenu_ctx *ctx)
+{
+    if (ctx->g1) cudaGraphExecDestroy(ctx->g1);
+    if (ctx->gN) cudaGraphExecDestroy(ctx->gN);
+    ctx->g1 = ctx->gN = nullptr;
+}
+
+}  // namespace
+
+extern "C" {
+
+void cosenu_params_default(cosenu_params *p)
+{
+    std::memset(p, 0, sizeof(*p));
+    p->nz = 2400;
+    p->nvz = 32;
+    p->gz = 4;
+    p->z0 = -600.0;
+    p->z1 = 600.0;
+    p->v0 = -1.0;
+    p->v1 = 1.0;
+    p->cfl = 0.4;
+    p->pmo = 1.0;
+    p->omega = 1e-2;
+    p->theta_deg = 37.0;
+    p->mu = 1.0;
+    p->scheme = COSENU_FV;
+    p->bc = COSENU_PERIODIC;
+    p->flags = COSENU_VAC | COSENU_COLL;
+    p->fd_advec = COSENU_FD_CENTER;
+    p->ko_order = 3;
+    p->precision = COSENU_FP64;
+}
+
+const char *cosenu_last_error(const cosenu_ctx *ctx)
+{
+    return ctx ? ctx->err.c_str() : g_create_error.c_str();
+}
+
+int cosenu_create(const cosenu_params *pp, cosenu_ctx **out)
+{
+    g_create_error.clear();
+    if (!pp || !out) {
+        g_create_error = "null argument";
+        return COSENU_ERR_ARG;
+    }
+    *out = nullptr;
+    const cosenu_params &p = *pp;
+    std::string why;
+    if (p.nz < 16 || p.nz % 8 != 0) why = "nz must be a multiple of 8 and >= 16";
+    else if (p.nvz < 1) why = "nvz must be >= 1";
+    else if (p.gz < 0 || p.gz > HP) why = "gz must be in [0, 16]";
+    else if (p.scheme != COSENU_FV && p.scheme != COSENU_FD) why = "unknown scheme";
+    else if (p.bc != COSENU_PERIODIC && p.bc != COSENU_OPEN) why = "unknown boundary";
+    else if (p.precision != COSENU_FP64 && p.precision != COSENU_FP32_BULK) why = "unknown precision";
+    else if (p.fd_advec < 0 || p.fd_advec > 2) why = "unknown FD advection stencil";
+    else if (p.ko_order != 3 && p.ko_order != 5) why = "ko_order must be 3 or 5";
+    else if (!(p.z1 > p.z0) || !(p.v1 > p.v0) || !(p.cfl > 0)) why = "empty box or non-positive CFL";
+    else if (p.tile_z != 0 && p.tile_z != 8 && p.tile_z != 16 && p.tile_z != 32) why = "tile_z must be 8, 16 or 32";
+    else if (p.tile_z != 0 && p.nz % p.tile_z != 0) why = "tile_z must divide nz";
+    else if (p.tile_v < 0 || p.tile_v > MAX_TV) why = "tile_v must be in [0, 256]";
+    if (!why.empty()) {
+        g_create_error = why;
+        return COSENU_ERR_ARG;
+    }
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+        g_create_error = "no CUDA device";
+        return COSENU_ERR_CUDA;
+    }
+    if (p.device < 0 || p.device >= ndev) {
+        g_create_error = "device ordinal out of range";
+        return COSENU_ERR_ARG;
+    }
+    cosenu_ctx *ctx = new cosenu_ctx();
+    ctx->p = p;
+    DeviceGuard dg(p.device);
+    ctx->fp32 = p.precision == COSENU_FP32_BULK;
+    ctx->ld = padded_ld(p.nz);
+    ctx->cs = (long long)p.nvz * ctx->ld;
+    ctx->H = std::max(4, p.gz);
+    choose_tile(ctx);
+    // grid exactly as NuOsc::NuOsc and set_vac_pars (src/nuosc.hpp:78-96,132-138)
+    ctx->dz = (p.z1 - p.z0) / p.nz;
+    ctx->dv = (p.v1 - p.v0) / (p.nvz);
+    ctx->dt = p.cfl * ctx->dz;
+    double th = p.theta_deg * M_PI / 180.0;
+    ctx->ct = (1.0 / 2.0) * p.omega * cos(2.0 * th);
+    ctx->st = (1.0 / 2.0) * p.omega * sin(2.0 * th);
+    ctx->h_Z.resize(p.nz);
+    ctx->h_Hm.resize(p.nz);
+    for (int j = 0; j < p.nz; ++j) {
+        ctx->h_Z[j] = p.z0 + (j + 0.5) * ctx->dz;
+        ctx->h_Hm[j] = -1.0e-3 * (ctx->h_Z[j] + 600.0);
+    }
+    ctx->h_vz.resize(p.nvz);
+    ctx->h_rowfac.resize(p.nvz);
+    for (int i = 0; i < p.nvz; ++i) {
+        double v = p.v0 + (i + 0.5) * ctx->dv;
+        ctx->h_vz[i] = v;
+        int sv = (0.0 < v) - (v < 0.0);
+        double f;
+        if (p.scheme == COSENU_FV) f = -v / ctx->dz;                       // rhs_fv.hpp:145
+        else if (p.fd_advec == COSENU_FD_CENTER) f = -v / (12 * ctx->dz);  // rhs_fd.hpp:57
+        else if (p.fd_advec == COSENU_FD_UPWIND) f = -sv * v / (12 * ctx->dz);
+        else f = sv * v / (12 * ctx->dz);
+        ctx->h_rowfac[i] = f;
+    }
+
+    int rc;
+    const size_t plane = (size_t)ctx->cs * sizeof(double);
+    const size_t state = plane * NCOMP;
+    const size_t ustate = ctx->fp32 ? state / 2 : state;
+    const size_t mom = (size_t)ctx->nvt * NMOM * p.nz * sizeof(double);
+#define AL(ptr, n)                                                              \
+    if ((rc = alloc(ctx, (void **)&(ptr), (n))) != COSENU_OK) {                 \
+        g_create_error = ctx->err;                                              \
+        cosenu_destroy(ctx);                                                    \
+        return rc;                                                              \
+    }
+    AL(ctx->Y, state);
+    AL(ctx->A, state);
+    AL(ctx->S0, state);
+    AL(ctx->U0, ustate);
+    AL(ctx->U1, ustate);
+    AL(ctx->G, plane);
+    AL(ctx->bG, plane);
+    for (int k = 0; k < 3; ++k) AL(ctx->M[k], mom);
+    AL(ctx->vz, p.nvz * sizeof(double));
+    AL(ctx->rowfac, p.nvz * sizeof(double));
+    AL(ctx->Hm, p.nz * sizeof(double));
+    AL(ctx->diag_part, (size_t)diag_blocks() * diag_slots() * sizeof(double));
+    AL(ctx->diag_out, 16 * sizeof(double));
+    AL(ctx->pee, 2 * (size_t)p.nvz * sizeof(double));
+    AL(ctx->tmp, (2 * (size_t)p.nvz + 2 * (size_t)p.nz) * sizeof(double));
+#undef AL
+    auto bail = [&](void) {
+        g_create_error = ctx->err;
+        cosenu_destroy(ctx);
+    };
+    cudaError_t e;
+    if ((e = cudaStreamCreateWithFlags(&ctx->own_stream, cudaStreamNonBlocking)) != cudaSuccess ||
+        (e = cudaMallocHost((void **)&ctx->h_pinned, 4096 + 2 * (size_t)p.nvz * 8)) != cudaSuccess) {
+        ctx->err = cudaGetErrorString(e);
+        bail();
+        return COSENU_ERR_CUDA;
+    }
+    ctx->stream = ctx->own_stream;
+    // zero everything once so ghost pads and unused partials are defined
+    for (void *q : {(void *)ctx->Y, (void *)ctx->A, (void *)ctx->S0, ctx->U0, ctx->U1})
+        cudaMemsetAsync(q, 0, q == ctx->U0 || q == ctx->U1 ? ustate : state, ctx->stream);
+    cudaMemsetAsync(ctx->G, 0, plane, ctx->stream);
+    cudaMemsetAsync(ctx->bG, 0, plane, ctx->stream);
+    for (int k = 0; k < 3; ++k) cudaMemsetAsync(ctx->M[k], 0, mom, ctx->stream);
+    cudaMemcpyAsync(ctx->vz, ctx->h_vz.data(), p.nvz * 8, cudaMemcpyHostToDevice, ctx->stream);
+    cudaMemcpyAsync(ctx->rowfac, ctx->h_rowfac.data(), p.nvz * 8, cudaMemcpyHostToDevice,
+                    ctx->stream);
+    cudaMemcpyAsync(ctx->Hm, ctx->h_Hm.data(), p.nz * 8, cudaMemcpyHostToDevice, ctx->stream);
+    if ((e = cudaStreamSynchronize(ctx->stream)) != cudaSuccess) {
+        ctx->err = cudaGetErrorString(e);
+        bail();
+        return COSENU_ERR_CUDA;
+    }
+    const char *ng = getenv("COSENU_NO_GRAPH");
+    ctx->use_graphs = !(ng && ng[0] == '1');
+    *out = ctx;
+    return COSENU_OK;
+}
+
+int cosenu_destroy(cosenu_ctx *ctx)
+{
+    if (!ctx) return COSENU_OK;
+    DeviceGuard dg(ctx->p.device);
+    if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+    drop_graphs(ctx);
+    void *bufs[] = {ctx->Y, ctx->A, ctx->S0, ctx->U0, ctx->U1, ctx->G, ctx->bG, ctx->M[0],
+                    ctx->M[1], ctx->M[2], ctx->vz, ctx->rowfac, ctx->Hm, ctx->diag_part,
+                    ctx->diag_out, ctx->pee, ctx->tmp};
+    for (void *b : bufs)
+        if (b) cudaFree(b);
+    if (ctx->h_pinned) cudaFreeHost(ctx->h_pinned);
+    if (ctx->own_stream) cudaStreamDestroy(ctx->own_stream);
+    delete ctx;
+    return COSENU_OK;
+}
+
+int cosenu_set_vac_pars(cosenu_ctx *ctx, double pmo, double omega, double theta_deg)
+{
+    if (!ctx) return COSENU_ERR_ARG;
+    DeviceGuard dg(ctx->p.device);
+    CK(cudaStreamSynchronize(ctx->stream));
+    ctx->p.pmo = pmo;
+    ctx->p.omega = omega;
+    ctx->p.theta_deg = theta_deg;
+    double th = theta_deg * M_PI / 180.0;
+    ctx->ct = (1.0 / 2.0) * omega * cos(2.0 * th);
+    ctx->st = (1.0 / 2.0) * omega * sin(2.0 * th);
+    drop_graphs(ctx);
+    return COSENU_OK;
+}
+
+int cosenu_set_collective_pars(cosenu_ctx *ctx, double mu)
+{
+    if (!ctx) return COSENU_ERR_ARG;
+    DeviceGuard dg(ctx->p.device);
+    CK(cudaStreamSynchronize(ctx->stream));
+    ctx->p.mu = mu;
+    drop_graphs(ctx);
+    return COSENU_OK;
+}
+
+int cosenu_set_stream(cosenu_ctx *ctx, void *stream)
+{
+    if (!ctx) return COSENU_ERR_ARG;
+    ctx->stream = stream ? (cudaStream_t)stream : ctx->own_stream;
+    return COSENU_OK;
+}
+
+int cosenu_grid(const cosenu_ctx *ctx, double out[5])
+{
+    if (!ctx || !out) return COSENU_ERR_ARG;
+    out[0] = ctx->dz;
+    out[1] = ctx->dv;
+    out[2] = ctx->dt;
+    out[3] = ctx->ct;
+    out[4] = ctx->st;
+    return COSENU_OK;
+}
+
+int cosenu_upload(cosenu_ctx *ctx, const double *const comp[8], int gz)
+{
+    if (!ctx || !comp) return COSENU_ERR_ARG;
+    if (gz < 0 || gz > HP) return fail(ctx, COSENU_ERR_ARG, "gz must be in [0, 16]");
+    DeviceGuard dg(ctx->p.device);
+    int rc = copy_planes_h2d(ctx, ctx->Y, comp, NCOMP, gz);
+    if (rc) return rc;
+    return prepare_state(ctx);
+}
+
+int cosenu_upload_device(cosenu_ctx *ctx, const double *const comp[8], int ld)
+{
+    if (!ctx || !comp || ld < ctx->p.nz) return COSENU_ERR_ARG;
+    DeviceGuard dg(ctx->p.device);
+    for (int c = 0; c < NCOMP; ++c)
+        CK(cudaMemcpy2DAsync(ctx->Y + (long long)c * ctx->cs + HP, (size_t)ctx->ld * 8, comp[c],
+                             (size_t)ld * 8, (size_t)ctx->p.nz * 8, ctx->p.nvz,
+                             cudaMemcpyDeviceToDevice, ctx->stream));
+    return prepare_state(ctx);
+}
+
+int cosenu_download(cosenu_ctx *ctx, double *const comp[8], int gz)
+{
+    if (!ctx || !comp) return COSENU_ERR_ARG;
+    if (!ctx->have_state) return fail(ctx, COSENU_ERR_STATE, "no state uploaded");
+    if (ctx->next_stage != 0) return fail(ctx, COSENU_ERR_STATE, "RK4 step in progress");
+    if (gz < 0 || gz > ctx->H) return fail(ctx, COSENU_ERR_ARG, "gz larger than the device ghost zone");
+    DeviceGuard dg(ctx->p.device);
+    const int nz = ctx->p.nz;
+    for (int c = 0; c < NCOMP; ++c) {
+        if (!comp[c]) return fail(ctx, COSENU_ERR_ARG, "null component pointer");
+        CK(cudaMemcpy2DAsync(comp[c], (size_t)(nz + 2 * gz) * 8,
+                             ctx->Y + (long long)c * ctx->cs + HP - gz, (size_t)ctx->ld * 8,
+                             (size_t)(nz + 2 * gz) * 8, ctx->p.nvz, cudaMemcpyDeviceToHost,
+                             ctx->stream));
+    }
+    CK(cudaStreamSynchronize(ctx->stream));
+    return COSENU_OK;
+}
+
+int cosenu_download_device(cosenu_ctx *ctx, double *const comp[8], int ld)
+{
+    if (!ctx || !comp || ld < ctx->p.nz) return COSENU_ERR_ARG;
+    if (!ctx->have_state) return fail(ctx, COSENU_ERR_STATE, "no state uploaded");
+    DeviceGuard dg(ctx->p.device);
+    for (int c = 0; c < NCOMP; ++c)
+        CK(cudaMemcpy2DAsync(comp[c], (size_t)ld * 8, ctx->Y + (long long)c * ctx->cs + HP,
+                             (size_t)ctx->ld * 8, (size_t)ctx->p.nz * 8, ctx->p.nvz,
+                             cudaMemcpyDeviceToDevice, ctx->stream));
+    return COSENU_OK;
+}
+
+int cosenu_set_profile(cosenu_ctx *ctx, const double *G, const double *bG, int gz)
+{
+    if (!ctx || !G || !bG) return COSENU_ERR_ARG;
+    if (gz < 0 || gz > HP) return fail(ctx, COSENU_ERR_ARG, "gz must be in [0, 16]");
+    DeviceGuard dg(ctx->p.device);
+    const double *g[1] = {G}, *bg[1] = {bG};
+    int rc = copy_planes_h2d(ctx, ctx->G, g, 1, gz);
+    if (!rc) rc = copy_planes_h2d(ctx, ctx->bG, bg, 1, gz);
+    if (rc) return rc;
+    ctx->have_profile = true;
+    return COSENU_OK;
+}
+
+int cosenu_set_state0(cosenu_ctx *ctx, const double *const comp[8], int gz)
+{
+    if (!ctx || !comp) return COSENU_ERR_ARG;
+    if (gz < 0 || gz > HP) return fail(ctx, COSENU_ERR_ARG, "gz must be in [0, 16]");
+    DeviceGuard dg(ctx->p.device);
+    int rc = copy_planes_h2d(ctx, ctx->S0, comp, NCOMP, gz);
+    if (rc) return rc;
+    ctx->have_state0 = true;
+    return COSENU_OK;
+}
+
+int cosenu_mark_state0(cosenu_ctx *ctx)
+{
+    if (!ctx) return COSENU_ERR_ARG;
+    if (!ctx->have_state) return fail(ctx, COSENU_ERR_STATE, "no state uploaded");
+    DeviceGuard dg(ctx->p.device);
+    CK(cudaMemcpyAsync(ctx->S0, ctx->Y, (size_t)ctx->cs * 8 * NCOMP, cudaMemcpyDeviceToDevice,
+                       ctx->stream));
+    ctx->have_state0 = true;
+    return COSENU_OK;
+}
+
+int cosenu_step_stage(cosenu_ctx *ctx, int stage)
+{
+    if (!ctx) return COSENU_ERR_ARG;
+    if (!ctx->have_state) return fail(ctx, COSENU_ERR_STATE, "no state uploaded");
+    if (stage != ctx->next_stage) return fail(ctx, COSENU_ERR_STATE, "stages must run in order 0..3");
+    DeviceGuard dg(ctx->p.device);
+    CK(launch_stage(ctx, stage + 1, ctx->stream));
+    ctx->next_stage = (stage + 1) % 4;
+    if (ctx->next_stage == 0) ctx->steps++;
+    return COSENU_OK;
+}
+
+int cosenu_step(cosenu_ctx *ctx, int nsteps)
+{
+    if (!ctx || nsteps < 0) return COSENU_ERR_ARG;
+    if (!ctx->have_state) return fail(ctx, COSENU_ERR_STATE, "no state uploaded");
+    if (ctx->next_stage != 0) return fail(ctx, COSENU_ERR_STATE, "RK4 step in progress");
+    if (nsteps == 0) return COSENU_OK;
+    DeviceGuard dg(ctx->p.device);
+    if (!ctx->use_graphs || nsteps == 1) {
+        CK(launch_steps(ctx, nsteps, ctx->stream));
+    } else {
+        if (!ctx->g1) CK(capture(ctx, 1, &ctx->g1));
+        if (nsteps >= GRAPH_CHUNK && !ctx->gN) CK(capture(ctx, GRAPH_CHUNK, &ctx->gN));
+        int n = nsteps;
+        while (n >= GRAPH_CHUNK) {
+            CK(cudaGraphLaunch(ctx->gN, ctx->stream));
+            n -= GRAPH_CHUNK;
+        }
+        while (n-- > 0) CK(cudaGraphLaunch(ctx->g1, ctx->stream));
+    }
+    ctx->steps += nsteps;
+    return COSENU_OK;
+}
+
+int cosenu_synchronize(cosenu_ctx *ctx)
+{
+    if (!ctx) return COSENU_ERR_ARG;
+    DeviceGuard dg(ctx->p.device);
+    CK(cudaStreamSynchronize(ctx->stream));
+    return COSENU_OK;
+}
+
+int cosenu_time(const cosenu_ctx *ctx, double *phy_time, long long *steps)
+{
+    if (!ctx) return COSENU_ERR_ARG;
+    if (phy_time) *phy_time = (double)ctx->steps * ctx->dt;
+    if (steps) *steps = ctx->steps;
+    return COSENU_OK;
+}
+
+int cosenu_analyse(cosenu_ctx *ctx, cosenu_diag *out)
+{
+    if (!ctx || !out) return COSENU_ERR_ARG;
+    if (!ctx->have_state) return fail(ctx, COSENU_ERR_STATE, "no state uploaded");
+    if (!ctx->have_profile || !ctx->have_state0)
+        return fail(ctx, COSENU_ERR_STATE, "analysis needs set_profile and state0");
+    if (ctx->next_stage != 0) return fail(ctx, COSENU_ERR_STATE, "RK4 step in progress");
+    DeviceGuard dg(ctx->p.device);
+    CK(launch_diag(ctx->Y, ctx->S0, ctx->G, ctx->bG, ctx->cs, ctx->ld, ctx->p.nz, ctx->p.nvz,
+                   ctx->dz, ctx->dv, ctx->diag_part, ctx->diag_out, ctx->stream));
+    CK(cudaMemcpyAsync(ctx->h_pinned, ctx->diag_out, 13 * 8, cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    const double *r = ctx->h_pinned;
+    out->dP_max = r[0];
+    out->avdP = r[1];
+    out->avbdP = r[2];
+    out->M0 = r[3];
+    out->M0_e1 = r[4];
+    out->M0_e2 = r[5];
+    out->M0_e3 = r[6];
+    out->Pee = r[7];
+    out->Pbee = r[8];
+    out->trace = r[9];
+    out->btrace = r[10];
+    out->eln = r[11];
+    if (r[12] != 0.0) return fail(ctx, COSENU_ERR_NONFINITE, "non-finite values in the state");
+    return COSENU_OK;
+}
+
+int cosenu_pee_v(cosenu_ctx *ctx, double *pee, double *pbee)
+{
+    if (!ctx || !pee || !pbee) return COSENU_ERR_ARG;
+    if (!ctx->have_state || !ctx->have_state0) return fail(ctx, COSENU_ERR_STATE, "needs state and state0");
+    if (ctx->next_stage != 0) return fail(ctx, COSENU_ERR_STATE, "RK4 step in progress");
+    DeviceGuard dg(ctx->p.device);
+    const int nvz = ctx->p.nvz;
+    CK(launch_pee_v(ctx->Y, ctx->S0, ctx->cs, ctx->ld, ctx->p.nz, nvz, ctx->pee, ctx->stream));
+    CK(cudaMemcpyAsync(ctx->h_pinned + 16, ctx->pee, 2 * (size_t)nvz * 8, cudaMemcpyDeviceToHost,
+                       ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    std::memcpy(pee, ctx->h_pinned + 16, nvz * 8);
+    std::memcpy(pbee, ctx->h_pinned + 16 + nvz, nvz * 8);
+    return COSENU_OK;
+}
+
+int cosenu_init_seeded(cosenu_ctx *ctx, uint64_t seed, uint32_t instance, double sig_nu,
+                       double sig_nubar, double alpha, double amp)
+{
+    if (!ctx) return COSENU_ERR_ARG;
+    if (!(sig_nu > 0) || !(sig_nubar > 0) || !(amp >= 0) || !(amp <= 1))
+        return fail(ctx, COSENU_ERR_ARG, "sigma must be > 0 and amp in [0, 1]");
+    DeviceGuard dg(ctx->p.device);
+    const int nvz = ctx->p.nvz;
+    std::vector<double> tab(2 * nvz);
+    for (int i = 0; i < nvz; ++i) {
+        tab[i] = gprof(ctx->h_vz[i], 1.0, sig_nu);
+        tab[nvz + i] = alpha * gprof(ctx->h_vz[i], 1.0, sig_nubar);
+    }
+    CK(cudaMemcpyAsync(ctx->tmp, tab.data(), 2 * nvz * 8, cudaMemcpyHostToDevice, ctx->stream));
+    CK(launch_init_seeded(ctx->Y, ctx->G, ctx->bG, ctx->tmp, ctx->tmp + nvz, ctx->cs, ctx->ld,
+                          ctx->p.nz, nvz, seed, instance, amp, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));  // tab goes out of scope
+    int rc = prepare_state(ctx);
+    if (rc) return rc;
+    ctx->have_profile = true;
+    ctx->steps = 0;
+    return cosenu_mark_state0(ctx);
+}
+
+int cosenu_init_reference(cosenu_ctx *ctx, double perturbation_size)
+{
+    if (!ctx) return COSENU_ERR_ARG;
+    DeviceGuard dg(ctx->p.device);
+    const int nvz = ctx->p.nvz, nz = ctx->p.nz;
+    const double signu = 0.6, sigbnu = 0.6, alpha = 0.90;  // src/initialize.hpp:12-14
+    std::vector<double> tab(2 * nvz + 2 * nz);
+    for (int i = 0; i < nvz; ++i) {
+        tab[i] = gprof(ctx->h_vz[i], 1.0, signu);
+        tab[nvz + i] = alpha * gprof(ctx->h_vz[i], 1.0, sigbnu);
+    }
+    for (int j = 0; j < nz; ++j) {
+        double z = ctx->h_Z[j];
+        double e = perturbation_size * exp(-(z - 0.0) * (z - 0.0) / 50.0);  // eps()
+        tab[2 * nvz + j] = e;
+        tab[2 * nvz + nz + j] = sqrt(1.0 - e * e);  // eps_()
+    }
+    CK(cudaMemcpyAsync(ctx->tmp, tab.data(), tab.size() * 8, cudaMemcpyHostToDevice, ctx->stream));
+    CK(launch_init_reference(ctx->Y, ctx->G, ctx->bG, ctx->tmp, ctx->tmp + nvz,
+                             ctx->tmp + 2 * nvz, ctx->tmp + 2 * nvz + nz, ctx->cs, ctx->ld, nz,
+                             nvz, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    int rc = prepare_state(ctx);
+    if (rc) return rc;
+    ctx->have_profile = true;
+    ctx->steps = 0;
+    return cosenu_mark_state0(ctx);
+}
+
+int cosenu_device_state(cosenu_ctx *ctx, double *comp[8], int *ld)
+{
+    if (!ctx || !comp) return COSENU_ERR_ARG;
+    for (int c = 0; c < NCOMP; ++c) comp[c] = ctx->Y + (long long)c * ctx->cs + HP;
+    if (ld) *ld = ctx->ld;
+    return COSENU_OK;
+}
+
+int cosenu_launches_per_step(const cosenu_ctx *ctx) { return ctx ? 4 : 0; }
+
+int cosenu_tile(const cosenu_ctx *ctx, int *tile_z, int *tile_v)
+{
+    if (!ctx) return COSENU_ERR_ARG;
+    if (tile_z) *tile_z = ctx->tz;
+    if (tile_v) *tile_v = ctx->tv;
+    return COSENU_OK;
+}
+
+int cosenu_device_bytes(const cosenu_ctx *ctx, size_t *bytes)
+{
+    if (!ctx || !bytes) return COSENU_ERR_ARG;
+    *bytes = ctx->bytes;
+    return COSENU_OK;
+}
+
+}  // extern "C"

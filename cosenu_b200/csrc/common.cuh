@@ -1,0 +1,54 @@
+// Shared definitions of the B200 kernels for COSEnu's RK4 path.
+//
+// Device layout of one state buffer: 8 component planes, each nvz rows of
+// `ld` cells; the interior cell (v, z) of component c sits at
+//     c*cs + v*ld + HP + z,   cs = nvz*ld,   ld = round_up(nz + 2*HP, 16).
+// HP = 16 cells (128 B) of padding on each side of a row keeps the interior
+// start of every row 128-byte aligned and holds the ghost cells (up to HP of
+// them) that the stencils read.  This is the reference's FieldVar layout
+// (v-major rows, z contiguous, src/nuosc.hpp:145-148) with a wider,
+// aligned ghost zone.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace cosenu {
+
+constexpr int NCOMP = 8;
+constexpr int HP = 16;         // pad cells per row side
+constexpr int NTHREADS = 256;  // threads per stage block
+constexpr int MAX_TV = 256;    // max v rows per tile
+constexpr int NMOM = 6;        // velocity moments per z
+
+enum Comp { EE = 0, XX, EXR, EXI, BEE, BXX, BEXR, BEXI };
+enum Scheme { FV = 0, FD = 1 };
+enum Flags { F_VAC = 1, F_MAT = 2, F_COLL = 4, F_ADVEC_OFF = 8 };
+
+// Arguments of one RK4 stage launch (passed by value).
+struct StageArgs {
+    const void *X;       // stage input (U or Y), TIN, with ghosts
+    const double *Y;     // RK4 base state (stages 2, 3)
+    double *A;           // RK4 accumulator
+    void *U;             // stage output, TOUT (U', U'' or the new Y)
+    const double *Min;   // [nvt][6][nz] per-v-tile moments of X
+    double *Mout;        // [nvt][6][nz] per-v-tile moments of U
+    const double *vz;    // [nvz] velocities
+    const double *rowfac;// [nvz] advection factor per row (scheme specific)
+    const double *Hm;    // [nz] matter potential
+    long long cs;        // component stride (elements)
+    int nz, nvz, ld, tv, nvt;
+    int H;               // ghost cells written per side
+    int bc, flags, fd_advec, ko_order;
+    double dt, dv, mu, ct, st, pmo, ko_eps;
+};
+
+// Layout helpers shared by host and device code.
+__host__ __device__ inline long long dev_index(long long cs, int ld, int c, int v, int z)
+{
+    return (long long)c * cs + (long long)v * ld + HP + z;
+}
+
+inline int padded_ld(int nz) { return ((nz + 2 * HP + 15) / 16) * 16; }
+
+}  // namespace cosenu

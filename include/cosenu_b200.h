@@ -1,0 +1,207 @@
+/*
+ * cosenu_b200.h -- C ABI of the B200 time-stepping path for COSEnu.
+ *
+ * The reference advances its state with the C++ member call
+ * NuOsc::step_rk4() (src/nuosc.hpp:166 declaration, :320-348 body, called once
+ * per iteration from src/main.cpp:175-177) on host arrays owned by NuOsc
+ * (FieldVar, src/structures.hpp:5-37).  This header is the boundary that
+ * replaces that call: a context owns the state in GPU memory, host arrays in
+ * the reference's own layout go in and out, and the driver advances any number
+ * of RK4 steps between analysis and snapshot events.
+ *
+ * Conventions
+ *  - Every function returns COSENU_OK (0) or an error code; nothing calls
+ *    exit() (the reference exits on bad input, src/parser.hpp:220-243,
+ *    src/snaps.hpp:88-92).  cosenu_last_error() gives the message.
+ *  - Host arrays use the reference layout: one array per component,
+ *    v-major rows of length ld = nz + 2*gz, interior cell (i, j) at
+ *    i*ld + j + gz (NuOsc::idx, src/nuosc.hpp:145-148).  Component order is
+ *    ee, xx, ex_re, ex_im, bee, bxx, bex_re, bex_im (src/structures.hpp:6-13).
+ *  - Work is queued on the context's CUDA stream; functions that return host
+ *    data synchronise that stream first.
+ *  - One host thread per context.
+ */
+#ifndef COSENU_B200_H
+#define COSENU_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define COSENU_NCOMP 8
+#define COSENU_ABI_VERSION 1
+
+/* status codes */
+enum {
+    COSENU_OK = 0,
+    COSENU_ERR_ARG = 1,       /* invalid argument or unsupported combination   */
+    COSENU_ERR_CUDA = 2,      /* CUDA runtime error (message in last_error)    */
+    COSENU_ERR_STATE = 3,     /* call out of order (e.g. step before upload)   */
+    COSENU_ERR_NONFINITE = 4, /* NaN/Inf detected in the evolved state         */
+    COSENU_ERR_NOMEM = 5      /* device allocation failed                       */
+};
+
+/* scheme: src/presets.hpp FV / FD (manage.py:167-173) */
+enum { COSENU_FV = 0, COSENU_FD = 1 };
+/* boundary: PERIODIC_BC / OPEN_BC (src/nuosc.hpp:214-277) */
+enum { COSENU_PERIODIC = 0, COSENU_OPEN = 1 };
+/* physics switches: VAC_OSC_ON, MAT_OSC_ON, COLL_OSC_ON, ADVEC_OFF
+ * (src/rhs_fv.hpp:143-233, src/rhs_fd.hpp:31-126) */
+enum { COSENU_VAC = 1u, COSENU_MAT = 2u, COSENU_COLL = 4u, COSENU_ADVEC_OFF = 8u };
+/* FD advection stencil: ADVEC_CENTER_FD / ADVEC_UPWIND / lopsided
+ * (src/rhs_fd.hpp:53-73) */
+enum { COSENU_FD_CENTER = 0, COSENU_FD_UPWIND = 1, COSENU_FD_LOPSIDED = 2 };
+/* arithmetic: plain FP64, or FP32 stage values with FP64 velocity moments,
+ * RK4 accumulator and base state */
+enum { COSENU_FP64 = 0, COSENU_FP32_BULK = 1 };
+
+/* Simulation parameters.  Field meanings follow the job.config keys parsed by
+ * Params (src/parser.hpp:46-256) plus the compile-time switches of
+ * src/presets.hpp, which are run-time choices here. */
+typedef struct cosenu_params {
+    int nz, nvz;          /* grid (nz must be a multiple of 8)                   */
+    int gz;               /* ghost width of the HOST layout (job.config "gz")    */
+    double z0, z1;        /* spatial box                                          */
+    double v0, v1;        /* velocity range                                       */
+    double cfl;           /* dt = CFL*dz (src/nuosc.hpp:80)                       */
+    double pmo, omega;    /* vacuum: mass ordering, omega (set_vac_pars)          */
+    double theta_deg;     /* mixing angle in DEGREES (src/nuosc.hpp:135)          */
+    double mu;            /* collective strength (set_collective_pars)            */
+    int scheme;           /* COSENU_FV / COSENU_FD                                */
+    int bc;               /* COSENU_PERIODIC / COSENU_OPEN                        */
+    unsigned flags;       /* COSENU_VAC | COSENU_MAT | COSENU_COLL | ...          */
+    int fd_advec;         /* COSENU_FD_* (FD only)                                */
+    int ko_order;         /* 3 (KO_ORD_3) or 5 (FD only)                          */
+    int precision;        /* COSENU_FP64 / COSENU_FP32_BULK                       */
+    int device;           /* CUDA device ordinal                                  */
+    int tile_z, tile_v;   /* kernel tile (0 = choose automatically)              */
+} cosenu_params;
+
+/* Fills p with the defaults of src/presets.hpp (periodic FV, vacuum and
+ * collective terms on) and the grid of cosenu_configs.yaml. */
+void cosenu_params_default(cosenu_params *p);
+
+typedef struct cosenu_ctx cosenu_ctx;
+
+/* Replaces NuOsc::NuOsc(Params) (src/nuosc.hpp:47-118) together with
+ * set_vac_pars / set_collective_pars (src/nuosc.hpp:132-143): validates the
+ * parameters and allocates the device state. */
+int cosenu_create(const cosenu_params *p, cosenu_ctx **out);
+
+/* Replaces NuOsc::~NuOsc (src/nuosc.hpp:119-130). */
+int cosenu_destroy(cosenu_ctx *ctx);
+
+/* Message of the last error on this context ("" if none); with ctx == NULL,
+ * the last error of a failed cosenu_create on this thread. */
+const char *cosenu_last_error(const cosenu_ctx *ctx);
+
+/* NuOsc::set_vac_pars (src/nuosc.hpp:132-139, theta in degrees) and
+ * NuOsc::set_collective_pars (src/nuosc.hpp:141-144): change the vacuum and
+ * collective parameters of an existing context. */
+int cosenu_set_vac_pars(cosenu_ctx *ctx, double pmo, double omega, double theta_deg);
+int cosenu_set_collective_pars(cosenu_ctx *ctx, double mu);
+
+/* Uses the given cudaStream_t for all later work (NULL: the context's own
+ * stream).  The stream must belong to the context's device. */
+int cosenu_set_stream(cosenu_ctx *ctx, void *cuda_stream);
+
+/* Grid values the reference derives in its constructor (src/nuosc.hpp:78-96):
+ * out = {dz, dv, dt, ct, st}. */
+int cosenu_grid(const cosenu_ctx *ctx, double out[5]);
+
+/* Host -> device copy of the evolved state v_stat (the arrays that
+ * NuOsc::read_state / initialize fill, src/snaps.hpp:75-124).  comp[c] points
+ * at component c in the reference layout with ghost width gz (>= 0).  Ghost
+ * cells on the device are refilled (updateBufferZone, src/nuosc.hpp:212-278). */
+int cosenu_upload(cosenu_ctx *ctx, const double *const comp[8], int gz);
+
+/* Device -> host copy of the evolved state into the reference layout
+ * (interior and gz ghost cells per side, as updateBufferZone would leave
+ * them).  Synchronises. */
+int cosenu_download(cosenu_ctx *ctx, double *const comp[8], int gz);
+
+/* Initial angular profiles G0 (Profile, src/structures.hpp:116-130; read by
+ * NuOsc::read_G0, src/snaps.hpp:153-183) used by the analysis. */
+int cosenu_set_profile(cosenu_ctx *ctx, const double *G, const double *bG, int gz);
+
+/* The initial state v_stat0 the analysis compares against (src/main.cpp:129-151).
+ * cosenu_mark_state0 takes the current device state instead (no host copy). */
+int cosenu_set_state0(cosenu_ctx *ctx, const double *const comp[8], int gz);
+int cosenu_mark_state0(cosenu_ctx *ctx);
+
+/* Replaces `nsteps` calls of NuOsc::step_rk4() (src/nuosc.hpp:320-348): each
+ * RK4 step is four fused stage kernels (ghost fill, right-hand side of
+ * src/rhs_fv.hpp or src/rhs_fd.hpp, stage combine).  Asynchronous. */
+int cosenu_step(cosenu_ctx *ctx, int nsteps);
+
+/* One RK4 stage (stage = 0..3, in order) -- the same kernels as cosenu_step,
+ * exposed so that a caller can time the stages separately. */
+int cosenu_step_stage(cosenu_ctx *ctx, int stage);
+
+/* Waits for the context's stream. */
+int cosenu_synchronize(cosenu_ctx *ctx);
+
+/* Simulated time and number of completed RK4 steps (NuOsc::phy_time). */
+int cosenu_time(const cosenu_ctx *ctx, double *phy_time, long long *steps);
+
+/* Diagnostics of src/analysis.hpp, reduced on the device. */
+typedef struct cosenu_diag {
+    double dP_max;  /* max over cells of |d|P|| and |d|bP||  (dcon, :108-125)     */
+    double avdP;    /* sum |d|P|| G / sum G                                        */
+    double avbdP;   /* sum |d|bP|| bG / sum bG                                     */
+    double M0;      /* |M0|                              (cal_Mn n = 0, :50-67)   */
+    double M0_e1, M0_e2, M0_e3;
+    double Pee;     /* sum ee / sum ee0                   (surv_prob, :169-182)   */
+    double Pbee;    /* sum bee / sum bee0                                          */
+    double trace;   /* sum (ee + xx) dz dv  (conserved)                            */
+    double btrace;  /* sum (bee + bxx) dz dv  (conserved)                          */
+    double eln;     /* sum (ee - bee) dz dv                                        */
+} cosenu_diag;
+
+/* Replaces NuOsc::analyse + surv_prob (src/analysis.hpp:3-25, 134-185)
+ * without copying the state to the host.  Needs set_profile and state0.
+ * Synchronises.  Returns COSENU_ERR_NONFINITE if the state holds NaN/Inf. */
+int cosenu_analyse(cosenu_ctx *ctx, cosenu_diag *out);
+
+/* Angle-resolved survival probabilities P_ee(v) = sum_z ee / sum_z ee0 and
+ * the same for nubar (arrays of nvz). Synchronises. */
+int cosenu_pee_v(cosenu_ctx *ctx, double *pee, double *pbee);
+
+/* On-device initial conditions.  cosenu_init_seeded: G = g(v,1,sig_nu),
+ * bG = alpha*g(v,1,sig_nubar) (g of src/miscellaneous_funcs.hpp:57-62) and a
+ * per-cell Philox-4x32-10 draw of (Re, Im) ex in [-amp, amp] for nu and nubar,
+ * shaped like src/initialize.hpp:30-38.  cosenu_init_reference: the
+ * reference's own NuOsc::initialize() (src/initialize.hpp:6-47).  Both set
+ * the profile and state0 as well and reset the time to zero. */
+int cosenu_init_seeded(cosenu_ctx *ctx, uint64_t seed, uint32_t instance, double sig_nu,
+                       double sig_nubar, double alpha, double amp);
+int cosenu_init_reference(cosenu_ctx *ctx, double perturbation_size);
+
+/* Device addresses of the evolved state for zero-copy use (e.g. from a
+ * framework tensor): comp[c] points at interior cell (0,0) of component c,
+ * rows are `ld` elements apart.  Valid until the next cosenu_* call that
+ * steps.  The pointed-to type is double (COSENU_FP64 and FP32_BULK keep the
+ * base state in FP64). */
+int cosenu_device_state(cosenu_ctx *ctx, double *comp[8], int *ld);
+
+/* Device <-> device variants of upload/download: comp[c] are device
+ * pointers with row pitch `ld` elements, interior only. */
+int cosenu_upload_device(cosenu_ctx *ctx, const double *const comp[8], int ld);
+int cosenu_download_device(cosenu_ctx *ctx, double *const comp[8], int ld);
+
+/* Number of kernel launches one cosenu_step(ctx, 1) issues. */
+int cosenu_launches_per_step(const cosenu_ctx *ctx);
+
+/* Tile shape in use (z cells x v rows per thread block). */
+int cosenu_tile(const cosenu_ctx *ctx, int *tile_z, int *tile_v);
+
+/* Bytes of device memory held by the context. */
+int cosenu_device_bytes(const cosenu_ctx *ctx, size_t *bytes);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* COSENU_B200_H */

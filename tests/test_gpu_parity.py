@@ -1,0 +1,228 @@
+"""Parity of the CUDA path (through the C ABI) with the reference.
+
+Tolerances (max-abs per component, FP64): <= 1e-10 before saturation
+against the reference's own outputs (tests/golden) and against the CPU oracle;
+<= 1e-6 on survival probabilities and the conservation diagnostics after
+saturation.  Measured differences are far smaller (1e-14 and below).
+"""
+import os
+
+import numpy as np
+import pytest
+
+from tests._util import gpu_from_case, load_golden, maxabs_per_comp, with_ghosts
+
+pytestmark = pytest.mark.gpu
+
+SMALL = ["fv_small", "fv_vac", "fv_oddv", "fd_small", "fd_vac", "fv_open", "fd_open", "fv_mat",
+         "fd_mat", "fd_ko5", "fv_advoff", "fd_advoff"]
+TOL_PRE = 1e-10
+TOL_POST = 1e-6
+NTHREADS = os.cpu_count() or 1
+
+
+def _inputs(case, d, oracle):
+    st0 = with_ghosts(case, d["state0"], oracle)
+    G = with_ghosts(case, d["G"][None], oracle)[0]
+    bG = with_ghosts(case, d["bG"][None], oracle)[0]
+    return st0, G, bG
+
+
+def _interior(case, a):
+    return a[..., case.gz:case.gz + case.nz]
+
+
+@pytest.mark.parametrize("name", SMALL)
+def test_snapshots_match_reference(gpu_lib, oracle, name):
+    """Every rho_<t>.dat the reference wrote, to <= 1e-10 max-abs."""
+    case, d = load_golden(name)
+    st0, G, bG = _inputs(case, d, oracle)
+    with gpu_from_case(case) as sim:
+        sim.upload(st0)
+        t_prev = 0
+        for t in d["dump_steps"]:
+            sim.evolve(int(t) - t_prev)
+            t_prev = int(t)
+            got = _interior(case, sim.download())
+            err = maxabs_per_comp(got, d[f"rho_{t}"])
+            assert np.all(err <= TOL_PRE), (name, int(t), err)
+
+
+@pytest.mark.parametrize("name", ["fv_small", "fd_small", "fv_vac", "fd_vac", "fv_open",
+                                  "fd_ko5", "fv_mat"])
+def test_analysis_matches_reference_tables(gpu_lib, oracle, name):
+    """conserved_quantities.dat / survival_probability.dat rows."""
+    case, d = load_golden(name)
+    st0, G, bG = _inputs(case, d, oracle)
+    with gpu_from_case(case) as sim:
+        sim.upload(st0)
+        sim.set_profile(G, bG)
+        sim.set_state0(st0)
+        t_prev = 0
+        for row, row_sp in zip(d["conserved_quantities"], d["survival_probability"]):
+            t = int(row[0])
+            sim.evolve(t - t_prev)
+            t_prev = t
+            a = sim.analyse()
+            got = np.array([a["dP_max"], a["avdP"], a["avbdP"], a["M0"]])
+            assert np.all(np.abs(got - row[1:]) <= 1e-12 * np.abs(row[1:]) + 1e-16), (t, got, row)
+            assert abs(a["Pee"] - row_sp[1]) <= 5e-7 * row_sp[1]
+            assert abs(a["Pbee"] - row_sp[2]) <= 5e-7 * row_sp[2]
+
+
+@pytest.mark.parametrize("tile", [(8, 1), (8, 3), (8, 32), (16, 5), (16, 16), (32, 7), (32, 16)])
+@pytest.mark.parametrize("name", ["fv_vac", "fd_vac", "fv_open", "fd_open"])
+def test_tile_shapes_against_oracle(gpu_lib, oracle, name, tile):
+    """Any tile shape, including v tiles that do not divide nvz."""
+    case, d = load_golden(name)
+    st0, G, bG = _inputs(case, d, oracle)
+    ref = oracle.step(case, st0, 10)
+    with gpu_from_case(case, tile_z=tile[0], tile_v=tile[1]) as sim:
+        assert sim.tile() == tile
+        sim.upload(st0)
+        sim.evolve(10)
+        got = sim.download()
+    err = maxabs_per_comp(_interior(case, got), _interior(case, ref))
+    assert np.all(err <= 1e-12), err
+    # ghost cells as updateBufferZone leaves them
+    assert np.abs(got - ref).max() <= 1e-12
+
+
+def test_deterministic_and_graph_equals_stagewise(gpu_lib, oracle):
+    case, d = load_golden("fv_vac")
+    st0, _, _ = _inputs(case, d, oracle)
+    outs = []
+    for mode in ("graph", "graph", "stages"):
+        with gpu_from_case(case) as sim:
+            sim.upload(st0)
+            if mode == "graph":
+                sim.evolve(37)
+            else:
+                for _ in range(37):
+                    for s in range(4):
+                        sim.step_stage(s)
+            outs.append(sim.download())
+    assert np.array_equal(outs[0], outs[1])
+    assert np.array_equal(outs[0], outs[2])
+
+
+def test_device_initial_conditions_bitwise(gpu_lib, oracle):
+    """On-device seeded and reference initial conditions equal the host
+    recipes bit for bit."""
+    case, d = load_golden("c1_pre")
+    G, bG, st = oracle.init_seeded(case, seed=int(d["seed"]))
+    with gpu_from_case(case) as sim:
+        sim.init_seeded(int(d["seed"]))
+        got = sim.download()
+    assert np.array_equal(_interior(case, got), _interior(case, st))
+    case, d = load_golden("fv_default_ic")
+    with gpu_from_case(case) as sim:
+        sim.initialize(float(d["perturbation_size"]))
+        got = sim.download()
+    assert np.array_equal(np.moveaxis(_interior(case, got), 0, -1), d["state0"])
+
+
+def _c1(oracle, name):
+    case, d = load_golden(name)
+    G, bG, st0 = oracle.init_seeded(case, seed=int(d["seed"]))
+    return case, d, G, bG, st0
+
+
+def test_c1_pre_saturation_500_steps(gpu_lib, oracle):
+    """configs[0] as specified (FV WENO7, 1024 x 64, 500 steps): against the
+    reference run (subset, checksums, analysis rows) and the full oracle
+    state, <= 1e-10 max-abs per component."""
+    case, d, G, bG, st0 = _c1(oracle, "c1_pre")
+    with gpu_from_case(case) as sim:
+        sim.init_seeded(int(d["seed"]))
+        t_prev = 0
+        for row, row_sp in zip(d["conserved_quantities"], d["survival_probability"]):
+            t = int(row[0])
+            sim.evolve(t - t_prev)
+            t_prev = t
+            a = sim.analyse()
+            assert abs(a["M0"] - row[4]) <= 1e-10
+            assert abs(a["dP_max"] - row[1]) <= 1e-10
+            assert abs(a["Pee"] - row_sp[1]) <= 5e-7 and abs(a["Pbee"] - row_sp[2]) <= 5e-7
+        got = _interior(case, sim.download())
+        pee, pbee = sim.pee_v()
+    err = maxabs_per_comp(got[:, :, ::16], d["rho_500_subset"])
+    assert np.all(err <= TOL_PRE), err
+    ck = np.stack([got.sum(axis=(1, 2)), (got * got).sum(axis=(1, 2)),
+                   np.abs(got).sum(axis=(1, 2))], 1)
+    assert np.allclose(ck, d["rho_500_checksums"], rtol=1e-10, atol=1e-14)
+    assert np.abs(pee - d["rho_500_pee_v"]).max() <= 1e-10
+    ref = oracle.step(case, st0, 500, nthreads=NTHREADS)
+    err = maxabs_per_comp(got, _interior(case, ref))
+    assert np.all(err <= TOL_PRE), err
+
+
+def test_c1_after_saturation_1500_steps(gpu_lib, oracle):
+    """The configs[0] grid through saturation: <Pee>, <Pbee>, |M0|, max dP and
+    P_ee(v) against the reference run at every analysis step, <= 1e-6."""
+    case, d, G, bG, st0 = _c1(oracle, "c1_sat")
+    worst = 0.0
+    with gpu_from_case(case) as sim:
+        sim.init_seeded(int(d["seed"]))
+        t_prev = 0
+        for row, row_sp in zip(d["conserved_quantities"], d["survival_probability"]):
+            t = int(row[0])
+            sim.evolve(t - t_prev)
+            t_prev = t
+            a = sim.analyse()
+            for got, want in ((a["Pee"], row_sp[1]), (a["Pbee"], row_sp[2]), (a["M0"], row[4]),
+                              (a["dP_max"], row[1]), (a["avdP"], row[2]), (a["avbdP"], row[3])):
+                worst = max(worst, abs(got - want))
+        pee, pbee = sim.pee_v()
+    assert d["survival_probability"][-1][1] < 0.9  # the run did saturate
+    assert worst <= TOL_POST, worst
+    assert np.abs(pee - d["rho_1500_pee_v"]).max() <= TOL_POST
+    assert np.abs(pbee - d["rho_1500_pbee_v"]).max() <= TOL_POST
+
+
+def test_c2_full_size_one_step_and_conservation(gpu_lib, oracle):
+    """configs[1] grid (FD, 32768 x 256): one step at full size against the
+    oracle, then trace conservation over further steps."""
+    from oracle.oracle import Case
+    case = Case(nz=32768, nvz=256, gz=2, z0=-3000.0, z1=3000.0, scheme="fd", pmo=1.0,
+                omega=1e-3, theta_deg=1e-6, mu=1.0)
+    G, bG, st0 = oracle.init_seeded(case, seed=7)
+    ref = oracle.step(case, st0, 1, nthreads=NTHREADS)
+    with gpu_from_case(case) as sim:
+        sim.init_seeded(7)
+        sim.evolve(1)
+        got = sim.download()
+        err = maxabs_per_comp(_interior(case, got), _interior(case, ref))
+        assert np.all(err <= 1e-12), err
+        a0 = sim.analyse()
+        sim.evolve(50)
+        a1 = sim.analyse()
+    assert abs(a1["trace"] - a0["trace"]) <= 1e-12 * abs(a0["trace"])
+    assert abs(a1["btrace"] - a0["btrace"]) <= 1e-12 * abs(a0["btrace"])
+
+
+def test_errors_are_reported_not_fatal(gpu_lib, oracle):
+    from cosenu_b200 import NuOsc
+    from cosenu_b200._lib import CosenuError, ERR_ARG, ERR_STATE, ERR_NONFINITE
+    with pytest.raises(CosenuError) as e:
+        NuOsc(nz=60, nvz=8)
+    assert e.value.code == ERR_ARG
+    case, d = load_golden("fv_small")
+    st0, G, bG = _inputs(case, d, oracle)
+    with gpu_from_case(case) as sim:
+        with pytest.raises(CosenuError) as e:
+            sim.evolve(1)
+        assert e.value.code == ERR_STATE
+        bad = st0.copy()
+        bad[0, 3, case.gz + 5] = np.nan
+        sim.upload(bad)
+        sim.set_profile(G, bG)
+        sim.set_state0(st0)
+        sim.evolve(2)
+        with pytest.raises(CosenuError) as e:
+            sim.analyse()
+        assert e.value.code == ERR_NONFINITE
+        # the context stays usable
+        sim.upload(st0)
+        sim.evolve(2)
+        assert np.isfinite(sim.analyse()["M0"])

@@ -8,6 +8,8 @@
 #include <string>
 #include <vector>
 
+#include <cuda.h>
+
 #include "../../include/cosenu_b200.h"
 #include "common.cuh"
 
@@ -31,6 +33,14 @@ cudaError_t launch_init_seeded(double *Y, double *G, double *bG, const double *G
 cudaError_t launch_init_reference(double *Y, double *G, double *bG, const double *Gv,
                                   const double *bGv, const double *ez, const double *ez_,
                                   long long cs, int ld, int nz, int nvz, cudaStream_t s);
+int make_state_map(CUtensorMap *map, const void *base, int elem_bytes, int ld, int nvz,
+                   long long cs, int box_cells);
+int tma_box_x();
+int tma_box_tile();
+cudaError_t tma_prepare();
+cudaError_t launch_fd_stage_tma(const CUtensorMap &mX, const CUtensorMap &mY,
+                                const CUtensorMap &mA, const StageArgs &a, int stage, int fp32,
+                                int *err, int nblocks, cudaStream_t s);
 }  // namespace cosenu
 
 using namespace cosenu;
@@ -54,6 +64,11 @@ struct cosenu_ctx {
     // host mirrors
     std::vector<double> h_vz, h_rowfac, h_Hm, h_Z;
     double *h_pinned = nullptr;  // small pinned buffer for results
+    // TMA-pipelined FD path: tensor maps over Y, U0, U1 (input boxes) and Y, A
+    bool use_tma = false;
+    int nsm = 148;
+    CUtensorMap mY40, mU0_40, mU1_40, mY32, mA32;
+    int *err_flag = nullptr;  // device word set by bounded waits that expired
     // graphs of 1 and GRAPH_CHUNK steps
     cudaGraphExec_t g1 = nullptr, gN = nullptr;
     bool use_graphs = true;
@@ -120,6 +135,16 @@ int alloc(cosenu_ctx *ctx, void **p, size_t n)
 void choose_tile(cosenu_ctx *ctx)
 {
     const cosenu_params &p = ctx->p;
+    const char *kenv = getenv("COSENU_KERNEL");
+    bool force_ldg = kenv && std::string(kenv) == "ldg";
+    if (p.scheme == COSENU_FD && p.nz % 32 == 0 && p.tile_z == 0 && p.tile_v == 0 && !force_ldg) {
+        // TMA path: 32-cell z tiles spanning all rows
+        ctx->use_tma = true;
+        ctx->tz = 32;
+        ctx->tv = p.nvz;
+        ctx->nvt = 1;
+        return;
+    }
     int tz = p.tile_z;
     if (tz == 0) tz = (p.nz % 32 == 0) ? 32 : (p.nz % 16 == 0 ? 16 : 8);
     int rp = NTHREADS / tz;
@@ -174,7 +199,28 @@ StageArgs stage_args(const cosenu_ctx *ctx, int stage)
 cudaError_t launch_stage(cosenu_ctx *ctx, int stage, cudaStream_t s)
 {
     StageArgs a = stage_args(ctx, stage);
+    if (ctx->use_tma) {
+        const CUtensorMap &mX = stage == 1 ? ctx->mY40 : (stage == 3 ? ctx->mU1_40 : ctx->mU0_40);
+        int nblk = std::min(ctx->p.nz / tma_box_tile(), ctx->nsm);
+        return launch_fd_stage_tma(mX, ctx->mY32, ctx->mA32, a, stage, ctx->fp32, ctx->err_flag,
+                                   nblk, s);
+    }
     return launch_rk4_stage(a, ctx->p.scheme, stage, ctx->tz, ctx->fp32, s);
+}
+
+// Reads the device error word; non-zero means a bounded wait in a stage
+// kernel expired (the results of that launch are not to be trusted).
+int check_err_flag(cosenu_ctx *ctx)
+{
+    if (!ctx->use_tma) return COSENU_OK;
+    int h = 0;
+    CK(cudaMemcpyAsync(&h, ctx->err_flag, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    if (h != 0) {
+        ctx->err = "stage kernel pipeline wait timed out (code " + std::to_string(h) + ")";
+        return COSENU_ERR_CUDA;
+    }
+    return COSENU_OK;
 }
 
 cudaError_t launch_steps(cosenu_ctx *ctx, int n, cudaStream_t s)
@@ -366,6 +412,7 @@ int cosenu_create(const cosenu_params *pp, cosenu_ctx **out)
     AL(ctx->diag_out, 16 * sizeof(double));
     AL(ctx->pee, 2 * (size_t)p.nvz * sizeof(double));
     AL(ctx->tmp, (2 * (size_t)p.nvz + 2 * (size_t)p.nz) * sizeof(double));
+    AL(ctx->err_flag, 64);
 #undef AL
     auto bail = [&](void) {
         g_create_error = ctx->err;
@@ -394,6 +441,23 @@ int cosenu_create(const cosenu_params *pp, cosenu_ctx **out)
         bail();
         return COSENU_ERR_CUDA;
     }
+    cudaMemsetAsync(ctx->err_flag, 0, 64, ctx->stream);
+    if (ctx->use_tma) {
+        const int ub = ctx->fp32 ? 4 : 8, bx = tma_box_x(), bt = tma_box_tile();
+        int r = make_state_map(&ctx->mY40, ctx->Y, 8, ctx->ld, p.nvz, ctx->cs, bx);
+        if (!r) r = make_state_map(&ctx->mU0_40, ctx->U0, ub, ctx->ld, p.nvz, ctx->cs, bx);
+        if (!r) r = make_state_map(&ctx->mU1_40, ctx->U1, ub, ctx->ld, p.nvz, ctx->cs, bx);
+        if (!r) r = make_state_map(&ctx->mY32, ctx->Y, 8, ctx->ld, p.nvz, ctx->cs, bt);
+        if (!r) r = make_state_map(&ctx->mA32, ctx->A, 8, ctx->ld, p.nvz, ctx->cs, bt);
+        if (!r && tma_prepare() != cudaSuccess) r = -2;
+        if (r) {
+            // no tensor-map support: fall back to the register-tiled kernel
+            ctx->use_tma = false;
+            ctx->p.tile_z = ctx->p.tile_v = 0;
+            choose_tile(ctx);
+        }
+        cudaDeviceGetAttribute(&ctx->nsm, cudaDevAttrMultiProcessorCount, p.device);
+    }
     const char *ng = getenv("COSENU_NO_GRAPH");
     ctx->use_graphs = !(ng && ng[0] == '1');
     *out = ctx;
@@ -408,7 +472,7 @@ int cosenu_destroy(cosenu_ctx *ctx)
     drop_graphs(ctx);
     void *bufs[] = {ctx->Y, ctx->A, ctx->S0, ctx->U0, ctx->U1, ctx->G, ctx->bG, ctx->M[0],
                     ctx->M[1], ctx->M[2], ctx->vz, ctx->rowfac, ctx->Hm, ctx->diag_part,
-                    ctx->diag_out, ctx->pee, ctx->tmp};
+                    ctx->diag_out, ctx->pee, ctx->tmp, ctx->err_flag};
     for (void *b : bufs)
         if (b) cudaFree(b);
     if (ctx->h_pinned) cudaFreeHost(ctx->h_pinned);
@@ -497,7 +561,7 @@ int cosenu_download(cosenu_ctx *ctx, double *const comp[8], int gz)
                              ctx->stream));
     }
     CK(cudaStreamSynchronize(ctx->stream));
-    return COSENU_OK;
+    return check_err_flag(ctx);
 }
 
 int cosenu_download_device(cosenu_ctx *ctx, double *const comp[8], int ld)
@@ -587,7 +651,7 @@ int cosenu_synchronize(cosenu_ctx *ctx)
     if (!ctx) return COSENU_ERR_ARG;
     DeviceGuard dg(ctx->p.device);
     CK(cudaStreamSynchronize(ctx->stream));
-    return COSENU_OK;
+    return check_err_flag(ctx);
 }
 
 int cosenu_time(const cosenu_ctx *ctx, double *phy_time, long long *steps)
@@ -610,6 +674,7 @@ int cosenu_analyse(cosenu_ctx *ctx, cosenu_diag *out)
                    ctx->dz, ctx->dv, ctx->diag_part, ctx->diag_out, ctx->stream));
     CK(cudaMemcpyAsync(ctx->h_pinned, ctx->diag_out, 13 * 8, cudaMemcpyDeviceToHost, ctx->stream));
     CK(cudaStreamSynchronize(ctx->stream));
+    if (int rc = check_err_flag(ctx)) return rc;
     const double *r = ctx->h_pinned;
     out->dP_max = r[0];
     out->avdP = r[1];

@@ -1,0 +1,455 @@
+// TMA-pipelined RK4 stage kernel for the FD scheme (src/rhs_fd.hpp:6-148).
+//
+// Same arithmetic and epilogue as rk4_stage_kernel (stage.cu); what changes
+// is how the operands reach the SM.  Each block is persistent over z-tiles of
+// 32 cells that span all nvz rows.  One producer warp streams chunks of 8 rows
+// x (32 + 2*4) cells of all 8 components of the stage input, and the matching
+// 8 x 32 cells of Y and A, into a ring of NBUF shared-memory buffers with
+// cp.async.bulk.tensor (one 3-D tensor-map copy per operand and chunk, box
+// {cells, rows, components}); eight consumer warps take one row each, read
+// their stencil from shared memory and write the results with coalesced
+// stores.  Full/empty mbarriers order the ring.  With up to NBUF-1 chunks in
+// flight (~100 KB per SM) the kernel keeps HBM busy without depending on
+// occupancy, which the register-heavy FP64 right-hand side limits.
+//
+// Every wait is bounded in time (globaltimer): on expiry the kernel records a
+// code in *err and carries on along the same control path, so no barrier is
+// left waiting and the host reports the error.
+#include <cuda.h>
+
+#include "common.cuh"
+
+namespace cosenu {
+
+namespace tma {
+
+constexpr int TZ = 32;           // cells per tile (one warp lane each)
+constexpr int HALO = 4;          // cells each side in the input box
+constexpr int XW = TZ + 2 * HALO;
+constexpr int R = 8;             // rows per chunk = consumer warps
+constexpr int NCONS = R * 32;    // consumer threads
+constexpr int NTHR = NCONS + 32; // + producer warp
+constexpr unsigned long long WAIT_NS = 2000000000ull;  // 2 s per wait
+
+__device__ __forceinline__ uint32_t smem_u32(const void *p)
+{
+    return (uint32_t)__cvta_generic_to_shared(p);
+}
+
+__device__ __forceinline__ unsigned long long gtimer()
+{
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+__device__ __forceinline__ void mbar_init(uint64_t *bar, uint32_t count)
+{
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count));
+}
+
+__device__ __forceinline__ bool mbar_try(uint64_t *bar, uint32_t parity)
+{
+    uint32_t ok;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
+        " selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(ok)
+        : "r"(smem_u32(bar)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+
+// Bounded wait; returns false (and records `code`) when the time limit passes.
+__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity, int *err, int code)
+{
+    if (mbar_try(bar, parity)) return true;
+    const unsigned long long t0 = gtimer();
+    while (!mbar_try(bar, parity)) {
+        if (gtimer() - t0 > WAIT_NS) {
+            atomicCAS(err, 0, code);
+            return false;
+        }
+    }
+    return true;
+}
+
+__device__ __forceinline__ void mbar_arrive(uint64_t *bar)
+{
+    asm volatile("mbarrier.arrive.release.cta.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar))
+                 : "memory");
+}
+
+__device__ __forceinline__ void mbar_expect_tx(uint64_t *bar, uint32_t bytes)
+{
+    asm volatile("mbarrier.arrive.expect_tx.release.cta.shared::cta.b64 _, [%0], %1;" ::"r"(
+                     smem_u32(bar)),
+                 "r"(bytes)
+                 : "memory");
+}
+
+__device__ __forceinline__ void tma_load_3d(void *dst, const CUtensorMap *map, int x, int y, int z,
+                                            uint64_t *bar)
+{
+    asm volatile(
+        "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes"
+        " [%0], [%1, {%2, %3, %4}], [%5];" ::"r"(smem_u32(dst)),
+        "l"((uint64_t)map), "r"(x), "r"(y), "r"(z), "r"(smem_u32(bar))
+        : "memory");
+}
+
+__device__ __forceinline__ void consumer_sync()
+{
+    asm volatile("bar.sync 1, %0;" ::"n"(NCONS) : "memory");
+}
+
+template <class TIN, int STAGE> struct Layout {
+    static constexpr int XB = NCOMP * R * XW * (int)sizeof(TIN);
+    static constexpr int YB = (STAGE == 2 || STAGE == 3) ? NCOMP * R * TZ * 8 : 0;
+    static constexpr int AB = (STAGE >= 2) ? NCOMP * R * TZ * 8 : 0;
+    static constexpr int BUF = ((XB + YB + AB) + 127) / 128 * 128;
+};
+
+}  // namespace tma
+
+template <int STAGE, class TC, class TIN, class TOUT, int NBUF>
+__global__ void __launch_bounds__(tma::NTHR, 1)
+    fd_stage_tma_kernel(const __grid_constant__ CUtensorMap mX,
+                        const __grid_constant__ CUtensorMap mY,
+                        const __grid_constant__ CUtensorMap mA, const StageArgs a, int *err)
+{
+    using namespace tma;
+    using L = Layout<TIN, STAGE>;
+    extern __shared__ __align__(1024) unsigned char smem[];
+    uint64_t *full = reinterpret_cast<uint64_t *>(smem + NBUF * L::BUF);
+    uint64_t *empty = full + NBUF;
+    double(*s_mom)[NMOM][TZ] = reinterpret_cast<double(*)[NMOM][TZ]>(empty + NBUF);
+    double(*s_red)[NMOM][TZ] = s_mom + 2;
+
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int nzt = a.nz / TZ;
+    const int nch = (a.nvz + R - 1) / R;
+    const bool coll = (a.flags & F_COLL) != 0;
+    const bool advec = (a.flags & F_ADVEC_OFF) == 0;
+    const bool open_bc = a.bc != 0;
+
+    if (tid == 0) {
+        for (int b = 0; b < NBUF; ++b) {
+            tma::mbar_init(&full[b], 1);
+            tma::mbar_init(&empty[b], R);
+        }
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    __syncthreads();
+
+    if (warp == R) {
+        // ------------------------------------------------------------ producer
+        if (lane == 0) {
+            uint32_t it = 0;
+            for (int t = blockIdx.x; t < nzt; t += gridDim.x) {
+                const int z0 = t * TZ;
+                for (int ch = 0; ch < nch; ++ch, ++it) {
+                    const int b = it % NBUF;
+                    if (it >= (uint32_t)NBUF)
+                        tma::mbar_wait(&empty[b], ((it / NBUF) - 1) & 1, err, 1);
+                    unsigned char *buf = smem + b * L::BUF;
+                    tma::mbar_expect_tx(&full[b], L::XB + L::YB + L::AB);
+                    tma::tma_load_3d(buf, &mX, HP + z0 - HALO, ch * R, 0, &full[b]);
+                    if (L::YB) tma::tma_load_3d(buf + L::XB, &mY, HP + z0, ch * R, 0, &full[b]);
+                    if (L::AB)
+                        tma::tma_load_3d(buf + L::XB + L::YB, &mA, HP + z0, ch * R, 0, &full[b]);
+                }
+            }
+        }
+        return;
+    }
+
+    // ---------------------------------------------------------------- consumers
+    const double dt = a.dt;
+    const TC pmo = (TC)a.pmo, ct = (TC)a.ct, st = (TC)a.st, mudv = (TC)(a.mu * a.dv);
+    const TC ko_eps = (TC)a.ko_eps;
+    // moments of the stage input for the first tile
+    int k = 0;
+    if (coll && tid < NMOM * TZ && (int)blockIdx.x < nzt) {
+        const int m = tid / TZ, zz = tid % TZ;
+        s_mom[0][m][zz] = a.Min[(long long)m * a.nz + blockIdx.x * TZ + zz];
+    }
+    consumer_sync();
+
+    uint32_t it = 0;
+    for (int t = blockIdx.x; t < nzt; t += gridDim.x, ++k) {
+        const int z0 = t * TZ;
+        const int z = z0 + lane;
+        const int cur = k & 1;
+        // prefetch the next tile's input moments into a register
+        double mnext = 0.0;
+        const int tn = t + gridDim.x;
+        if (coll && tid < NMOM * TZ && tn < nzt)
+            mnext = a.Min[(long long)(tid / TZ) * a.nz + tn * TZ + tid % TZ];
+        double macc[NMOM] = {0, 0, 0, 0, 0, 0};
+        const double M0A = s_mom[cur][0][lane], M0B = s_mom[cur][1][lane],
+                     M0C = s_mom[cur][2][lane], M1A = s_mom[cur][3][lane],
+                     M1B = s_mom[cur][4][lane], M1C = s_mom[cur][5][lane];
+        const TC hm = (a.flags & F_MAT) ? (TC)a.Hm[z] : TC(0);
+
+        for (int ch = 0; ch < nch; ++ch, ++it) {
+            const int b = it % NBUF;
+            tma::mbar_wait(&full[b], (it / NBUF) & 1, err, 2);
+            const unsigned char *buf = smem + b * L::BUF;
+            const TIN *xs = reinterpret_cast<const TIN *>(buf) + warp * XW + HALO + lane;
+            const double *ys = reinterpret_cast<const double *>(buf + L::XB) + warp * TZ + lane;
+            const double *as = reinterpret_cast<const double *>(buf + L::XB + L::YB) + warp * TZ + lane;
+            const int v = ch * R + warp;
+            const bool valid = v < a.nvz;
+            const int vr = valid ? v : a.nvz - 1;
+            const double vzv = a.vz[vr];
+            const TC factor = (TC)a.rowfac[vr];
+            const int sv = (vzv > 0.0) - (vzv < 0.0);
+
+            TC c[NCOMP], adv[NCOMP], ko[NCOMP];
+            double x0[NCOMP];
+#pragma unroll
+            for (int q = 0; q < NCOMP; ++q) {
+                const TIN *p = xs + q * (R * XW);
+                x0[q] = (double)p[0];
+                c[q] = (TC)p[0];
+                const TC m2 = (TC)p[-2], m1 = (TC)p[-1], p1 = (TC)p[1], p2 = (TC)p[2];
+                adv[q] = TC(0);
+                if (advec) {
+                    if (a.fd_advec == 0) {
+                        adv[q] = factor * ((m2 - p2) - TC(8) * (m1 - p1));
+                    } else if (a.fd_advec == 1) {
+                        adv[q] = factor * (TC(-4) * (TC)p[-3 * sv] + TC(18) * (TC)p[-2 * sv] -
+                                           TC(36) * (TC)p[-sv] + TC(22) * c[q]);
+                    } else {
+                        adv[q] = factor * ((TC)p[-3 * sv] - TC(6) * (TC)p[-2 * sv] +
+                                           TC(18) * (TC)p[-sv] - TC(10) * c[q] - TC(3) * (TC)p[sv]);
+                    }
+                }
+                if (a.ko_order == 5)
+                    ko[q] = ko_eps * ((TC)p[-3] + (TC)p[3] - TC(6) * (m2 + p2) + TC(15) * (m1 + p1) -
+                                      TC(20) * c[q]);
+                else
+                    ko[q] = ko_eps * (m2 + p2 - TC(4) * (m1 + p1) + TC(6) * c[q]);
+            }
+            // right-hand side in the order of src/rhs_fd.hpp: vacuum, matter,
+            // advection, collective, dissipation
+            TC o[NCOMP];
+#pragma unroll
+            for (int q = 0; q < NCOMP; ++q) o[q] = TC(0);
+            if (a.flags & F_VAC) {
+                o[EE] = -pmo * TC(2) * st * c[EXI];
+                o[XX] = pmo * TC(2) * st * c[EXI];
+                o[EXR] = -pmo * TC(2) * ct * c[EXI];
+                o[EXI] = pmo * (TC(2) * ct * c[EXR] + st * (c[EE] - c[XX]));
+                o[BEE] = -pmo * TC(2) * st * c[BEXI];
+                o[BXX] = pmo * TC(2) * st * c[BEXI];
+                o[BEXR] = -pmo * TC(2) * ct * c[BEXI];
+                o[BEXI] = pmo * (TC(2) * ct * c[BEXR] + st * (c[BEE] - c[BXX]));
+            }
+            if (a.flags & F_MAT) {
+                o[EXR] += hm * c[EXI];
+                o[EXI] += -hm * c[EXR];
+                o[BEXR] += -hm * c[BEXI];
+                o[BEXI] += hm * c[BEXR];
+            }
+#pragma unroll
+            for (int q = 0; q < NCOMP; ++q) o[q] += adv[q];
+            if (coll) {
+                const TC SA = (TC)(M0A - vzv * M1A), SB = (TC)(M0B - vzv * M1B),
+                         SC = (TC)(M0C - vzv * M1C);
+                const TC Iee = TC(2) * (c[EXR] * SA - c[EXI] * SB);
+                const TC Ibee = TC(2) * (c[BEXR] * SA + c[BEXI] * SB);
+                o[EE] += mudv * Iee;
+                o[XX] += mudv * (-Iee);
+                o[EXR] += mudv * ((c[XX] - c[EE]) * SA + c[EXI] * SC);
+                o[EXI] += mudv * (-(c[XX] - c[EE]) * SB - c[EXR] * SC);
+                o[BEE] += mudv * Ibee;
+                o[BXX] += mudv * (-Ibee);
+                o[BEXR] += mudv * ((c[BXX] - c[BEE]) * SA - c[BEXI] * SC);
+                o[BEXI] += mudv * ((c[BXX] - c[BEE]) * SB + c[BEXR] * SC);
+            }
+#pragma unroll
+            for (int q = 0; q < NCOMP; ++q) o[q] += ko[q];
+
+            // stage combine
+            TOUT u[NCOMP];
+            double anew[NCOMP];
+#pragma unroll
+            for (int q = 0; q < NCOMP; ++q) {
+                const double kk = (double)o[q];
+                if (STAGE == 1) {
+                    u[q] = (TOUT)(x0[q] + (0.5 * dt) * kk);
+                    anew[q] = x0[q] + (dt / 6.0) * kk;
+                } else if (STAGE == 2 || STAGE == 3) {
+                    u[q] = (TOUT)(ys[q * R * TZ] + (STAGE == 2 ? 0.5 * dt : dt) * kk);
+                    anew[q] = as[q * R * TZ] + (dt / 3.0) * kk;
+                } else {
+                    u[q] = (TOUT)(as[q * R * TZ] + (dt / 6.0) * kk);
+                    anew[q] = 0.0;
+                }
+            }
+            // this warp is done with the buffer
+            __syncwarp();
+            if (lane == 0) tma::mbar_arrive(&empty[b]);
+
+            TOUT uleft[NCOMP];
+            if (open_bc) {
+#pragma unroll
+                for (int q = 0; q < NCOMP; ++q) uleft[q] = __shfl_sync(0xffffffffu, u[q], lane > 0 ? lane - 1 : 0);
+            }
+            if (valid) {
+                TOUT *U = static_cast<TOUT *>(a.U);
+                const long long ro = (long long)v * a.ld + HP;
+#pragma unroll
+                for (int q = 0; q < NCOMP; ++q) {
+                    TOUT *row = U + q * a.cs + ro;
+                    row[z] = u[q];
+                    if (STAGE <= 3) a.A[q * a.cs + ro + z] = anew[q];
+                    if (!open_bc) {
+                        if (z < a.H) row[z + a.nz] = u[q];
+                        if (z >= a.nz - a.H) row[z - a.nz] = u[q];
+                    } else {
+                        if (z == 0)
+                            for (int g = 1; g <= a.H; ++g) row[-g] = u[q];
+                        if (z == a.nz - 1) {
+                            TOUT p0 = uleft[q], p1 = u[q];
+                            for (int g = 0; g < a.H; ++g) {
+                                TOUT gh = p1 * TOUT(2) - p0;
+                                row[a.nz + g] = gh;
+                                p0 = p1;
+                                p1 = gh;
+                            }
+                        }
+                    }
+                }
+                if (coll) {
+                    const double Am = (double)u[EXI] + (double)u[BEXI];
+                    const double Bm = (double)u[EXR] - (double)u[BEXR];
+                    const double Cm = (double)u[EE] - (double)u[XX] - (double)u[BEE] + (double)u[BXX];
+                    macc[0] += Am;
+                    macc[1] += Bm;
+                    macc[2] += Cm;
+                    macc[3] += vzv * Am;
+                    macc[4] += vzv * Bm;
+                    macc[5] += vzv * Cm;
+                }
+            }
+        }
+        // tile epilogue: output moments (fixed-order sum over warps) and the
+        // next tile's input moments
+        if (coll) {
+#pragma unroll
+            for (int m = 0; m < NMOM; ++m) s_red[warp][m][lane] = macc[m];
+            consumer_sync();
+            if (tid < NMOM * TZ) {
+                const int m = tid / TZ, zz = tid % TZ;
+                double s = 0.0;
+#pragma unroll
+                for (int w = 0; w < R; ++w) s += s_red[w][m][zz];
+                a.Mout[(long long)m * a.nz + z0 + zz] = s;
+                s_mom[cur ^ 1][m][zz] = mnext;
+            }
+            consumer_sync();
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// host side
+
+typedef CUresult (*EncodeTiledFn)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *,
+                                  const cuuint64_t *, const cuuint64_t *, const cuuint32_t *,
+                                  const cuuint32_t *, CUtensorMapInterleave, CUtensorMapSwizzle,
+                                  CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+static EncodeTiledFn encode_fn()
+{
+    static EncodeTiledFn fn = nullptr;
+    if (!fn) {
+        void *p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) ==
+                cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = (EncodeTiledFn)p;
+    }
+    return fn;
+}
+
+// 3-D map over one 8-component buffer: (cells of a padded row, rows, components)
+int make_state_map(CUtensorMap *map, const void *base, int elem_bytes, int ld, int nvz,
+                   long long cs, int box_cells)
+{
+    EncodeTiledFn fn = encode_fn();
+    if (!fn) return -1;
+    cuuint64_t dims[3] = {(cuuint64_t)ld, (cuuint64_t)nvz, (cuuint64_t)NCOMP};
+    cuuint64_t strides[2] = {(cuuint64_t)ld * elem_bytes, (cuuint64_t)cs * elem_bytes};
+    cuuint32_t box[3] = {(cuuint32_t)box_cells, (cuuint32_t)tma::R, (cuuint32_t)NCOMP};
+    cuuint32_t es[3] = {1, 1, 1};
+    CUresult r = fn(map, elem_bytes == 8 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64
+                                         : CU_TENSOR_MAP_DATA_TYPE_FLOAT32,
+                    3, const_cast<void *>(base), dims, strides, box, es,
+                    CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                    CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    return r == CUDA_SUCCESS ? 0 : (int)r;
+}
+
+int tma_box_x() { return tma::XW; }
+int tma_box_tile() { return tma::TZ; }
+
+template <int STAGE, class TC, class TIN, class TOUT>
+static cudaError_t launch_one(const CUtensorMap &mX, const CUtensorMap &mY, const CUtensorMap &mA,
+                              const StageArgs &a, int *err, int nblocks, cudaStream_t s)
+{
+    using L = tma::Layout<TIN, STAGE>;
+    constexpr int NB = (L::BUF * 4 + 16 * 1024 <= 220 * 1024) ? 4 : 3;
+    const int shmem = NB * L::BUF + 2 * NB * 8 + (2 + tma::R) * NMOM * tma::TZ * 8;
+    auto kern = fd_stage_tma_kernel<STAGE, TC, TIN, TOUT, NB>;
+    if (nblocks <= 0) {  // preparation call: raise the dynamic shared-memory limit
+        return cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, shmem);
+    }
+    kern<<<nblocks, tma::NTHR, shmem, s>>>(mX, mY, mA, a, err);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_fd_stage_tma(const CUtensorMap &mX, const CUtensorMap &mY,
+                                const CUtensorMap &mA, const StageArgs &a, int stage, int fp32,
+                                int *err, int nblocks, cudaStream_t s);
+
+// Sets the shared-memory attribute of every instantiation on the current device.
+cudaError_t tma_prepare()
+{
+    CUtensorMap m{};
+    StageArgs a{};
+    for (int fp32 = 0; fp32 < 2; ++fp32)
+        for (int st = 1; st <= 4; ++st) {
+            cudaError_t e = launch_fd_stage_tma(m, m, m, a, st, fp32, nullptr, 0, nullptr);
+            if (e != cudaSuccess) return e;
+        }
+    return cudaSuccess;
+}
+
+cudaError_t launch_fd_stage_tma(const CUtensorMap &mX, const CUtensorMap &mY,
+                                const CUtensorMap &mA, const StageArgs &a, int stage, int fp32,
+                                int *err, int nblocks, cudaStream_t s)
+{
+    if (fp32) {
+        switch (stage) {
+        case 1: return launch_one<1, float, double, float>(mX, mY, mA, a, err, nblocks, s);
+        case 2: return launch_one<2, float, float, float>(mX, mY, mA, a, err, nblocks, s);
+        case 3: return launch_one<3, float, float, float>(mX, mY, mA, a, err, nblocks, s);
+        case 4: return launch_one<4, float, float, double>(mX, mY, mA, a, err, nblocks, s);
+        }
+    } else {
+        switch (stage) {
+        case 1: return launch_one<1, double, double, double>(mX, mY, mA, a, err, nblocks, s);
+        case 2: return launch_one<2, double, double, double>(mX, mY, mA, a, err, nblocks, s);
+        case 3: return launch_one<3, double, double, double>(mX, mY, mA, a, err, nblocks, s);
+        case 4: return launch_one<4, double, double, double>(mX, mY, mA, a, err, nblocks, s);
+        }
+    }
+    return cudaErrorInvalidValue;
+}
+
+}  // namespace cosenu

@@ -61,17 +61,21 @@ __device__ __forceinline__ bool mbar_try(uint64_t *bar, uint32_t parity)
 }
 
 // Bounded wait; returns false (and records `code`) when the time limit passes.
+// Once any wait in the grid has expired (*err != 0) later waits give up
+// at once, so a broken pipeline ends within one time limit.
 __device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity, int *err, int code)
 {
     if (mbar_try(bar, parity)) return true;
+    volatile int *verr = err;
+    if (*verr != 0) return false;
     const unsigned long long t0 = gtimer();
-    while (!mbar_try(bar, parity)) {
-        if (gtimer() - t0 > WAIT_NS) {
+    for (uint32_t n = 1;; ++n) {
+        if (mbar_try(bar, parity)) return true;
+        if ((n & 63) == 0 && (*verr != 0 || gtimer() - t0 > WAIT_NS)) {
             atomicCAS(err, 0, code);
             return false;
         }
     }
-    return true;
 }
 
 __device__ __forceinline__ void mbar_arrive(uint64_t *bar)

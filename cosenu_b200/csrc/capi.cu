@@ -45,7 +45,8 @@ cudaError_t launch_fd_stage_tma(const CUtensorMap &mX, const CUtensorMap &mY,
 
 using namespace cosenu;
 
-static thread_local std::string g_create_error;
+// message for cosenu_last_error(NULL): failures that have no context
+thread_local std::string g_create_error;
 
 struct cosenu_ctx {
     cosenu_params p{};

@@ -192,6 +192,24 @@ int cosenu_device_state(cosenu_ctx *ctx, double *comp[8], int *ld);
 int cosenu_upload_device(cosenu_ctx *ctx, const double *const comp[8], int ld);
 int cosenu_download_device(cosenu_ctx *ctx, double *const comp[8], int ld);
 
+/* For callers that must not allocate device memory (a host application whose
+ * device memory all comes from its own pool, or a loop that cannot afford the
+ * device synchronisation cudaMalloc/cudaFree may cause).  No counterpart in the
+ * reference.  Advances a state the caller holds in device memory by `nsteps`
+ * RK4 steps without any device allocation: state[c] points at component c,
+ * interior cell (v, z) at state[c][v*ld + z] (no ghost cells; ld >= nz), read
+ * and overwritten in place; p gives the grid and physics as for cosenu_create.
+ * Working memory is one fixed device array inside the library (20.5 MB, held by
+ * every GPU that loads the library until exit): grids need
+ * nvz * (nz + 32 rounded up to a multiple of 16) <= 69632 and nz <= 16384
+ * (the configs[0] grid, 1024 x 64, fits); larger grids return COSENU_ERR_ARG
+ * with the limit in cosenu_last_error(NULL).  The first call on a device looks
+ * up that array's address; make it before any stream capture.  Calls share the
+ * array, so calls whose GPU work overlaps race; order them.  Work is queued on
+ * `stream` (a cudaStream_t, NULL for the default stream) and not waited for. */
+int cosenu_step_noalloc(const cosenu_params *p, double *const state[8], int ld, int nsteps,
+                        void *stream);
+
 /* Number of kernel launches one cosenu_step(ctx, 1) issues. */
 int cosenu_launches_per_step(const cosenu_ctx *ctx);
 

@@ -40,12 +40,30 @@ sys.path.insert(0, ROOT)
 
 METRIC = "cell-updates/s (nz*nvz*RK4 steps), FP64"
 UNIT = "cell-updates/s"
-WORKLOAD = dict(nz=32768, nvz=256, gz=2, z0=-3000.0, z1=3000.0, v0=-1.0, v1=1.0, cfl=0.4,
-                pmo=1.0, omega=1e-3, theta_deg=1e-6, mu=1.0, scheme="fd")
+# FD at scale (the headline); configs[0]: FV WENO7 small; configs[2]:
+# FV at 65536 x 512 (FP32-bulk form, FP64 for comparison)
+WORKLOADS = {
+    "c2": dict(nz=32768, nvz=256, gz=2, z0=-3000.0, z1=3000.0, v0=-1.0, v1=1.0, cfl=0.4,
+               pmo=1.0, omega=1e-3, theta_deg=1e-6, mu=1.0, scheme="fd"),
+    "c1": dict(nz=1024, nvz=64, gz=4, z0=-600.0, z1=600.0, v0=-1.0, v1=1.0, cfl=0.4,
+               pmo=1.0, omega=0.0, theta_deg=0.0, mu=1.0, scheme="fv"),
+    "c3": dict(nz=65536, nvz=512, gz=4, z0=-600.0, z1=600.0, v0=-1.0, v1=1.0, cfl=0.4,
+               pmo=1.0, omega=0.0, theta_deg=0.0, mu=1.0, scheme="fv"),
+}
+WORKLOAD_NAMES = {
+    "c2": "FD (central FD4 + KO3) RK4, nz 32768 x nvz 256, periodic, mu 1, omega 1e-3, "
+          "theta 1e-6 deg",
+    "c1": "FV WENO7 RK4, nz 1024 x nvz 64, periodic, mu 1, omega 0",
+    "c3": "FV WENO7 RK4, nz 65536 x nvz 512, periodic, mu 1, omega 0",
+}
+WORKLOAD = dict(WORKLOADS["c2"])
 IC = dict(sig_nu=0.6, sig_nubar=0.5, alpha=0.9, amp=1e-6)
 SEED = 20240601
 ANAL_EVERY = 40  # manage.py: N_ITER = 4000 steps, n_analyze = 100
 PASSES = (3, 5, 5, 3)  # state passes (x 64 B) per cell of stages 1..4
+# algorithmic bytes per cell of stages 1..4: FP64 (U in FP64) and FP32-bulk
+# (U in FP32, Y and A in FP64)
+STAGE_BYTES = {"fp64": (192, 320, 320, 192), "fp32": (160, 256, 256, 160)}
 FALLBACK_HBM_GBS = 6650.0
 
 
@@ -161,7 +179,7 @@ def run_ours(args):
 
     stream = torch.cuda.Stream()
     torch.cuda.set_stream(stream)
-    sim = NuOsc(device=local, **WORKLOAD)
+    sim = NuOsc(device=local, precision=args.precision, **WORKLOAD)
     sim.set_stream(stream.cuda_stream)
     cells = WORKLOAD["nz"] * WORKLOAD["nvz"]
     sim.init_seeded(SEED + rank, **IC)
@@ -235,20 +253,27 @@ def run_ours(args):
     if rank == 0:
         peak, peak_src = peak_hbm()
         dom = 1  # stage 2 (5 passes), same kernel shape as stage 3
-        algo_bytes = PASSES[dom] * 64 * cells
+        sb = STAGE_BYTES[args.precision]
+        algo_bytes = sb[dom] * cells
         achieved = algo_bytes / (stage_ms[dom] / 1e3) / 1e9
         tr = traffic_from_profile()
-        traffic = tr.get("fd_stage2_bytes_per_launch") if tr else None
+        key = f"{args.workload}_{args.precision}_stage2_bytes_per_launch"
+        traffic = tr.get(key) if (tr and WORKLOAD["nz"] == WORKLOADS[args.workload]["nz"]) else None
         cpu = cpu_baseline(args) if (world == 1 and not args.no_cpu_baseline) else None
+        buf_mb = 8 * WORKLOAD["nvz"] * (WORKLOAD["nz"] + 32) * 8 / 1e6
+        sch = WORKLOAD["scheme"].upper()
         result = {
-            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": K,
+            "metric": METRIC if args.precision == "fp64" else METRIC.replace("FP64", "FP32-bulk"),
+            "value": value, "unit": UNIT, "n_gpus": world, "steps": K,
             "warmup": args.warmup, "ms_per_step": total_ms / K, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": "FD (central FD4 + KO3) RK4, nz 32768 x nvz 256, periodic, "
-                                   "mu 1, omega 1e-3, theta 1e-6 deg",
-                       "nz": WORKLOAD["nz"], "nvz": WORKLOAD["nvz"], "scheme": "FD",
-                       "precision": "FP64", "tile": [tz, tv],
-                       "l2": "inputs larger than L2 (537 MB per state buffer)",
+            "scaling": "weak", "vs_baseline": None,
+            "dtype": "f64" if args.precision == "fp64" else "f32 (FP64 moments/accumulator/base)",
+            "data": "synthetic",
+            "config": {"workload": WORKLOAD_NAMES[args.workload], "name": args.workload,
+                       "nz": WORKLOAD["nz"], "nvz": WORKLOAD["nvz"], "scheme": sch,
+                       "precision": args.precision.upper(), "tile": [tz, tv],
+                       "l2": f"inputs larger than L2 ({buf_mb:.0f} MB per state buffer)"
+                             if buf_mb > 126 else "inputs fit in L2 (small case)",
                        "instances_per_gpu": 1},
             "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": d2h,
@@ -257,11 +282,11 @@ def run_ours(args):
             "gpu_launches": 4 * K,
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": traffic,
-                         "kernel": "rk4_stage_kernel<FD, stage 2> (5 state passes)",
+                         "kernel": f"rk4_stage_tma_kernel<{sch}, stage 2> (5 state passes)",
                          "algorithmic_bytes_per_launch": algo_bytes,
                          "avg_launch_ms": stage_ms[dom], "peak_source": peak_src},
             "stage_ms": stage_ms,
-            "step_hbm_frac": (1024 * cells / (total_ms / K / 1e3) / 1e9) / peak,
+            "step_hbm_frac": (sum(sb) * cells / (total_ms / K / 1e3) / 1e9) / peak,
             "clocks": clk.summary(),
             "cpu_baseline": cpu,
         }
@@ -276,7 +301,7 @@ def run_ours(args):
 # ---------------------------------------------------------------------------
 def _ref_exe():
     from oracle.build import ref_binary
-    exe = ref_binary("fd")
+    exe = ref_binary(WORKLOAD["scheme"])
     if not os.path.exists(exe):
         raise FileNotFoundError(exe)
     return exe
@@ -290,7 +315,7 @@ def _ref_run(nz_sample: int, nsteps: int, threads: int):
     dz = (w["z1"] - w["z0"]) / w["nz"]
     case = Case(nz=nz_sample, nvz=w["nvz"], gz=w["gz"], z0=-0.5 * nz_sample * dz,
                 z1=0.5 * nz_sample * dz, cfl=w["cfl"], pmo=w["pmo"], omega=w["omega"],
-                theta_deg=w["theta_deg"], mu=w["mu"], scheme="fd")
+                theta_deg=w["theta_deg"], mu=w["mu"], scheme=w["scheme"])
     o = Oracle()
     G, bG, st0 = o.init_seeded(case, seed=SEED, **IC)
     n_iter = max(nsteps + 1, 10)
@@ -314,7 +339,8 @@ def cpu_baseline(args, budget_s: float = 20.0):
         nz *= 2
     t, n = _ref_run(nz, 9, threads)
     return {"value": nz * nvz * n / t, "unit": UNIT, "cores": threads, "kind": "reference",
-            "sample": f"reference FD build (g++ -O3 -fopenmp, OMP_NUM_THREADS={threads}), "
+            "sample": f"reference {WORKLOAD['scheme'].upper()} build (g++ -O3 -fopenmp, "
+                      f"OMP_NUM_THREADS={threads}), "
                       f"{n} RK4 steps on a z-subset nz={nz} of the workload grid "
                       f"(same dz, nvz={nvz}, physics), loop time from its time.txt"}
 
@@ -342,15 +368,16 @@ def run_reference_arm(args):
         _ref_run(nz, max(W, 9), threads)
     t, n = _ref_run(nz, K, threads)
     value = nz * nvz * n / t
-    sample = (f"reference FD build (g++ -O3 -fopenmp, OMP_NUM_THREADS={threads}), {n} RK4 "
+    sample = (f"reference {WORKLOAD['scheme'].upper()} build (g++ -O3 -fopenmp, "
+              f"OMP_NUM_THREADS={threads}), {n} RK4 "
               f"steps on a z-subset nz={nz} of the workload grid (same dz, nvz={nvz}, physics); "
               "loop time from its time.txt")
     print(json.dumps({
         "metric": METRIC, "value": value, "unit": UNIT, "impl": "reference", "n_gpus": world,
         "steps": n, "warmup": W, "ms_per_step": t / n * 1e3, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": "FD (central FD4 + KO3) RK4, nz 32768 x nvz 256, periodic, "
-                               "mu 1, omega 1e-3, theta 1e-6 deg", "sample_nz": nz},
+        "config": {"workload": WORKLOAD_NAMES[args.workload], "name": args.workload,
+                   "sample_nz": nz},
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "reference",
                          "sample": sample},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
@@ -364,10 +391,18 @@ def main():
     ap.add_argument("--warmup", type=int, default=10)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--nz", type=int, default=WORKLOAD["nz"],
+    ap.add_argument("--workload", choices=sorted(WORKLOADS), default="c2",
+                    help="c2 (default, the headline): FD 32768 x 256; c1: FV 1024 x 64; "
+                         "c3: FV 65536 x 512")
+    ap.add_argument("--precision", choices=["fp64", "fp32"], default="fp64")
+    ap.add_argument("--nz", type=int, default=None,
                     help="smaller z extent at the same dz (profiling cases only; the headline "
                          "workload is nz = 32768)")
     args = ap.parse_args()
+    WORKLOAD.clear()
+    WORKLOAD.update(WORKLOADS[args.workload])
+    if args.nz is None:
+        args.nz = WORKLOAD["nz"]
     if args.nz != WORKLOAD["nz"]:
         dz = (WORKLOAD["z1"] - WORKLOAD["z0"]) / WORKLOAD["nz"]
         WORKLOAD.update(nz=args.nz, z0=-0.5 * args.nz * dz, z1=0.5 * args.nz * dz)

@@ -38,9 +38,10 @@ int make_state_map(CUtensorMap *map, const void *base, int elem_bytes, int ld, i
 int tma_box_x();
 int tma_box_tile();
 cudaError_t tma_prepare();
-cudaError_t launch_fd_stage_tma(const CUtensorMap &mX, const CUtensorMap &mY,
-                                const CUtensorMap &mA, const StageArgs &a, int stage, int fp32,
-                                int *err, int nblocks, cudaStream_t s);
+int tma_max_nvz();
+cudaError_t launch_rk4_stage_tma(const CUtensorMap &mX, const CUtensorMap &mY,
+                                 const CUtensorMap &mA, const StageArgs &a, int scheme, int stage,
+                                 int fp32, int *err, int nblocks, cudaStream_t s);
 }  // namespace cosenu
 
 using namespace cosenu;
@@ -138,7 +139,7 @@ void choose_tile(cosenu_ctx *ctx)
     const cosenu_params &p = ctx->p;
     const char *kenv = getenv("COSENU_KERNEL");
     bool force_ldg = kenv && std::string(kenv) == "ldg";
-    if (p.scheme == COSENU_FD && p.nz % 32 == 0 && p.tile_z == 0 && p.tile_v == 0 && !force_ldg) {
+    if (p.nz % 32 == 0 && p.nvz <= tma_max_nvz() && p.tile_z == 0 && p.tile_v == 0 && !force_ldg) {
         // TMA path: 32-cell z tiles spanning all rows
         ctx->use_tma = true;
         ctx->tz = 32;
@@ -203,8 +204,8 @@ cudaError_t launch_stage(cosenu_ctx *ctx, int stage, cudaStream_t s)
     if (ctx->use_tma) {
         const CUtensorMap &mX = stage == 1 ? ctx->mY40 : (stage == 3 ? ctx->mU1_40 : ctx->mU0_40);
         int nblk = std::min(ctx->p.nz / tma_box_tile(), ctx->nsm);
-        return launch_fd_stage_tma(mX, ctx->mY32, ctx->mA32, a, stage, ctx->fp32, ctx->err_flag,
-                                   nblk, s);
+        return launch_rk4_stage_tma(mX, ctx->mY32, ctx->mA32, a, ctx->p.scheme, stage, ctx->fp32,
+                                    ctx->err_flag, nblk, s);
     }
     return launch_rk4_stage(a, ctx->p.scheme, stage, ctx->tz, ctx->fp32, s);
 }

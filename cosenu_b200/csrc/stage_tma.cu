@@ -1,4 +1,5 @@
-// TMA-pipelined RK4 stage kernel for the FD scheme (src/rhs_fd.hpp:6-148).
+// TMA-pipelined RK4 stage kernel for the FV (src/rhs_fv.hpp:115-236) and FD
+// (src/rhs_fd.hpp:6-148) schemes.
 //
 // Same arithmetic and epilogue as rk4_stage_kernel (stage.cu); what changes
 // is how the operands reach the SM.  Each block is persistent over z-tiles of
@@ -12,12 +13,20 @@
 // flight (~100 KB per SM) the kernel keeps HBM busy without depending on
 // occupancy, which the register-heavy FP64 right-hand side limits.
 //
+// FV: a warp holds one row, so every lane reconstructs the upwind WENO7 face it
+// owns from the shared-memory stencil and takes its neighbour's face by
+// shuffle; the one face per row outside the tile (8 components) is computed by
+// lanes 0-7 in one extra round.  FD: the common variant of manage.py (central
+// FD4 + KO3) is a compile-time fast path; the upwind / lopsided / KO5 variants
+// take the generic path.
+//
 // Every wait is bounded in time (globaltimer): on expiry the kernel records a
 // code in *err and carries on along the same control path, so no barrier is
 // left waiting and the host reports the error.
 #include <cuda.h>
 
 #include "common.cuh"
+#include "weno.cuh"
 
 namespace cosenu {
 
@@ -116,11 +125,11 @@ template <class TIN, int STAGE> struct Layout {
 
 }  // namespace tma
 
-template <int STAGE, class TC, class TIN, class TOUT, int NBUF>
+template <int SCHEME, bool GEN, int STAGE, class TC, class TIN, class TOUT, int NBUF>
 __global__ void __launch_bounds__(tma::NTHR, 1)
-    fd_stage_tma_kernel(const __grid_constant__ CUtensorMap mX,
-                        const __grid_constant__ CUtensorMap mY,
-                        const __grid_constant__ CUtensorMap mA, const StageArgs a, int *err)
+    rk4_stage_tma_kernel(const __grid_constant__ CUtensorMap mX,
+                         const __grid_constant__ CUtensorMap mY,
+                         const __grid_constant__ CUtensorMap mA, const StageArgs a, int *err)
 {
     using namespace tma;
     using L = Layout<TIN, STAGE>;
@@ -129,6 +138,8 @@ __global__ void __launch_bounds__(tma::NTHR, 1)
     uint64_t *empty = full + NBUF;
     double(*s_mom)[NMOM][TZ] = reinterpret_cast<double(*)[NMOM][TZ]>(empty + NBUF);
     double(*s_red)[NMOM][TZ] = s_mom + 2;
+    double *s_vz = reinterpret_cast<double *>(s_red + R);  // [nvz] velocities
+    double *s_fac = s_vz + a.nvz;                          // [nvz] advection factors
 
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const int nzt = a.nz / TZ;
@@ -172,6 +183,10 @@ __global__ void __launch_bounds__(tma::NTHR, 1)
     const double dt = a.dt;
     const TC pmo = (TC)a.pmo, ct = (TC)a.ct, st = (TC)a.st, mudv = (TC)(a.mu * a.dv);
     const TC ko_eps = (TC)a.ko_eps;
+    for (int i = tid; i < a.nvz; i += NCONS) {
+        s_vz[i] = a.vz[i];
+        s_fac[i] = a.rowfac[i];
+    }
     // moments of the stage input for the first tile
     int k = 0;
     if (coll && tid < NMOM * TZ && (int)blockIdx.x < nzt) {
@@ -198,67 +213,114 @@ __global__ void __launch_bounds__(tma::NTHR, 1)
 
         for (int ch = 0; ch < nch; ++ch, ++it) {
             const int b = it % NBUF;
-            tma::mbar_wait(&full[b], (it / NBUF) & 1, err, 2);
-            const unsigned char *buf = smem + b * L::BUF;
-            const TIN *xs = reinterpret_cast<const TIN *>(buf) + warp * XW + HALO + lane;
-            const double *ys = reinterpret_cast<const double *>(buf + L::XB) + warp * TZ + lane;
-            const double *as = reinterpret_cast<const double *>(buf + L::XB + L::YB) + warp * TZ + lane;
             const int v = ch * R + warp;
             const bool valid = v < a.nvz;
             const int vr = valid ? v : a.nvz - 1;
-            const double vzv = a.vz[vr];
-            const TC factor = (TC)a.rowfac[vr];
-            const int sv = (vzv > 0.0) - (vzv < 0.0);
+            const double vzv = s_vz[vr];
+            const TC factor = (TC)s_fac[vr];
+            tma::mbar_wait(&full[b], (it / NBUF) & 1, err, 2);
+            const unsigned char *buf = smem + b * L::BUF;
+            const TIN *xrow = reinterpret_cast<const TIN *>(buf) + warp * XW + HALO;
+            const TIN *xs = xrow + lane;
+            const double *ys = reinterpret_cast<const double *>(buf + L::XB) + warp * TZ + lane;
+            const double *as = reinterpret_cast<const double *>(buf + L::XB + L::YB) + warp * TZ + lane;
 
-            TC c[NCOMP], adv[NCOMP], ko[NCOMP];
+            TC c[NCOMP], o[NCOMP];
             double x0[NCOMP];
 #pragma unroll
             for (int q = 0; q < NCOMP; ++q) {
-                const TIN *p = xs + q * (R * XW);
-                x0[q] = (double)p[0];
-                c[q] = (TC)p[0];
-                const TC m2 = (TC)p[-2], m1 = (TC)p[-1], p1 = (TC)p[1], p2 = (TC)p[2];
-                adv[q] = TC(0);
-                if (advec) {
-                    if (a.fd_advec == 0) {
-                        adv[q] = factor * ((m2 - p2) - TC(8) * (m1 - p1));
-                    } else if (a.fd_advec == 1) {
-                        adv[q] = factor * (TC(-4) * (TC)p[-3 * sv] + TC(18) * (TC)p[-2 * sv] -
-                                           TC(36) * (TC)p[-sv] + TC(22) * c[q]);
-                    } else {
-                        adv[q] = factor * ((TC)p[-3 * sv] - TC(6) * (TC)p[-2 * sv] +
-                                           TC(18) * (TC)p[-sv] - TC(10) * c[q] - TC(3) * (TC)p[sv]);
-                    }
+                x0[q] = (double)xs[q * (R * XW)];
+                c[q] = (TC)x0[q];
+            }
+            if (SCHEME == FV) {
+                // upwind flux difference (rhs_fv.hpp:143-162): this lane's face
+                // and its neighbour's; lanes 0-7 first build the row's edge faces
+                const int dir = (vzv >= 0.0) ? 1 : -1;
+                TC edge = TC(0);
+                if (advec && lane < NCOMP) {
+                    const TIN *pe = xrow + lane * (R * XW) + (dir > 0 ? -1 : TZ);
+                    edge = weno7_face((TC)pe[-3 * dir], (TC)pe[-2 * dir], (TC)pe[-dir], (TC)pe[0],
+                                      (TC)pe[dir], (TC)pe[2 * dir], (TC)pe[3 * dir]);
                 }
-                if (a.ko_order == 5)
-                    ko[q] = ko_eps * ((TC)p[-3] + (TC)p[3] - TC(6) * (m2 + p2) + TC(15) * (m1 + p1) -
-                                      TC(20) * c[q]);
-                else
-                    ko[q] = ko_eps * (m2 + p2 - TC(4) * (m1 + p1) + TC(6) * c[q]);
-            }
-            // right-hand side in the order of src/rhs_fd.hpp: vacuum, matter,
-            // advection, collective, dissipation
-            TC o[NCOMP];
+                const int src = min(max(lane - dir, 0), TZ - 1);
 #pragma unroll
-            for (int q = 0; q < NCOMP; ++q) o[q] = TC(0);
-            if (a.flags & F_VAC) {
-                o[EE] = -pmo * TC(2) * st * c[EXI];
-                o[XX] = pmo * TC(2) * st * c[EXI];
-                o[EXR] = -pmo * TC(2) * ct * c[EXI];
-                o[EXI] = pmo * (TC(2) * ct * c[EXR] + st * (c[EE] - c[XX]));
-                o[BEE] = -pmo * TC(2) * st * c[BEXI];
-                o[BXX] = pmo * TC(2) * st * c[BEXI];
-                o[BEXR] = -pmo * TC(2) * ct * c[BEXI];
-                o[BEXI] = pmo * (TC(2) * ct * c[BEXR] + st * (c[BEE] - c[BXX]));
-            }
-            if (a.flags & F_MAT) {
-                o[EXR] += hm * c[EXI];
-                o[EXI] += -hm * c[EXR];
-                o[BEXR] += -hm * c[BEXI];
-                o[BEXI] += hm * c[BEXR];
-            }
+                for (int q = 0; q < NCOMP; ++q) {
+                    TC adv = TC(0);
+                    if (advec) {
+                        const TIN *p = xs + q * (R * XW);
+                        const TC fown = weno7_face((TC)p[-3 * dir], (TC)p[-2 * dir], (TC)p[-dir],
+                                                   (TC)p[0], (TC)p[dir], (TC)p[2 * dir],
+                                                   (TC)p[3 * dir]);
+                        TC fnb = __shfl_sync(0xffffffffu, fown, src);
+                        const TC e = __shfl_sync(0xffffffffu, edge, q);
+                        if ((dir > 0 && lane == 0) || (dir < 0 && lane == TZ - 1)) fnb = e;
+                        if (open_bc) {
+                            // flux ghosts under OPEN_BC (updateBufferZone on rflux/lflux,
+                            // rhs_fv.hpp:118-119): rflux[-1] = rflux[0],
+                            // lflux[nz] = 2 lflux[nz-1] - lflux[nz-2]
+                            const TC fm1 = __shfl_sync(0xffffffffu, fown, lane > 0 ? lane - 1 : 0);
+                            if (dir > 0 && z == 0) fnb = fown;
+                            if (dir < 0 && z == a.nz - 1) fnb = fown * TC(2) - fm1;
+                        }
+                        adv = dir > 0 ? factor * (fown - fnb) : factor * (fnb - fown);
+                    }
+                    o[q] = adv;
+                }
+                if (a.flags & F_VAC) {
+                    o[EE] += TC(-2) * st * c[EXI] * pmo;
+                    o[XX] += TC(2) * st * c[EXI] * pmo;
+                    o[EXR] += TC(-2) * ct * c[EXI] * pmo;
+                    o[EXI] += (TC(2) * ct * c[EXR] + st * (c[EE] - c[XX])) * pmo;
+                    o[BEE] += TC(-2) * st * c[BEXI] * pmo;
+                    o[BXX] += TC(2) * st * c[BEXI] * pmo;
+                    o[BEXR] += TC(-2) * ct * c[BEXI] * pmo;
+                    o[BEXI] += (TC(2) * ct * c[BEXR] + st * (c[BEE] - c[BXX])) * pmo;
+                }
+                if (a.flags & F_MAT) {
+                    o[EXR] += hm * c[EXI];
+                    o[EXI] += -hm * c[EXR];
+                    o[BEXR] += -hm * c[BEXI];
+                    o[BEXI] += hm * c[BEXR];
+                }
+            } else {
+                // FD: vacuum, matter, advection, (collective below), dissipation
 #pragma unroll
-            for (int q = 0; q < NCOMP; ++q) o[q] += adv[q];
+                for (int q = 0; q < NCOMP; ++q) o[q] = TC(0);
+                if (a.flags & F_VAC) {
+                    o[EE] = -pmo * TC(2) * st * c[EXI];
+                    o[XX] = pmo * TC(2) * st * c[EXI];
+                    o[EXR] = -pmo * TC(2) * ct * c[EXI];
+                    o[EXI] = pmo * (TC(2) * ct * c[EXR] + st * (c[EE] - c[XX]));
+                    o[BEE] = -pmo * TC(2) * st * c[BEXI];
+                    o[BXX] = pmo * TC(2) * st * c[BEXI];
+                    o[BEXR] = -pmo * TC(2) * ct * c[BEXI];
+                    o[BEXI] = pmo * (TC(2) * ct * c[BEXR] + st * (c[BEE] - c[BXX]));
+                }
+                if (a.flags & F_MAT) {
+                    o[EXR] += hm * c[EXI];
+                    o[EXI] += -hm * c[EXR];
+                    o[BEXR] += -hm * c[BEXI];
+                    o[BEXI] += hm * c[BEXR];
+                }
+                const int sv = (vzv > 0.0) - (vzv < 0.0);
+#pragma unroll
+                for (int q = 0; q < NCOMP; ++q) {
+                    if (!advec) continue;
+                    const TIN *p = xs + q * (R * XW);
+                    const TC m2 = (TC)p[-2], m1 = (TC)p[-1], p1 = (TC)p[1], p2 = (TC)p[2];
+                    TC adv;
+                    if (!GEN || a.fd_advec == 0) {
+                        adv = factor * ((m2 - p2) - TC(8) * (m1 - p1));
+                    } else if (a.fd_advec == 1) {
+                        adv = factor * (TC(-4) * (TC)p[-3 * sv] + TC(18) * (TC)p[-2 * sv] -
+                                        TC(36) * (TC)p[-sv] + TC(22) * c[q]);
+                    } else {
+                        adv = factor * ((TC)p[-3 * sv] - TC(6) * (TC)p[-2 * sv] +
+                                        TC(18) * (TC)p[-sv] - TC(10) * c[q] - TC(3) * (TC)p[sv]);
+                    }
+                    o[q] += adv;
+                }
+            }
             if (coll) {
                 const TC SA = (TC)(M0A - vzv * M1A), SB = (TC)(M0B - vzv * M1B),
                          SC = (TC)(M0C - vzv * M1C);
@@ -273,8 +335,20 @@ __global__ void __launch_bounds__(tma::NTHR, 1)
                 o[BEXR] += mudv * ((c[BXX] - c[BEE]) * SA - c[BEXI] * SC);
                 o[BEXI] += mudv * ((c[BXX] - c[BEE]) * SB + c[BEXR] * SC);
             }
+            if (SCHEME == FD) {
 #pragma unroll
-            for (int q = 0; q < NCOMP; ++q) o[q] += ko[q];
+                for (int q = 0; q < NCOMP; ++q) {
+                    const TIN *p = xs + q * (R * XW);
+                    const TC m2 = (TC)p[-2], m1 = (TC)p[-1], p1 = (TC)p[1], p2 = (TC)p[2];
+                    TC ko;
+                    if (GEN && a.ko_order == 5)
+                        ko = ko_eps * ((TC)p[-3] + (TC)p[3] - TC(6) * (m2 + p2) + TC(15) * (m1 + p1) -
+                                       TC(20) * c[q]);
+                    else
+                        ko = ko_eps * (m2 + p2 - TC(4) * (m1 + p1) + TC(6) * c[q]);
+                    o[q] += ko;
+                }
+            }
 
             // stage combine
             TOUT u[NCOMP];
@@ -300,7 +374,8 @@ __global__ void __launch_bounds__(tma::NTHR, 1)
             TOUT uleft[NCOMP];
             if (open_bc) {
 #pragma unroll
-                for (int q = 0; q < NCOMP; ++q) uleft[q] = __shfl_sync(0xffffffffu, u[q], lane > 0 ? lane - 1 : 0);
+                for (int q = 0; q < NCOMP; ++q)
+                    uleft[q] = __shfl_sync(0xffffffffu, u[q], lane > 0 ? lane - 1 : 0);
             }
             if (valid) {
                 TOUT *U = static_cast<TOUT *>(a.U);
@@ -401,59 +476,74 @@ int make_state_map(CUtensorMap *map, const void *base, int elem_bytes, int ld, i
 
 int tma_box_x() { return tma::XW; }
 int tma_box_tile() { return tma::TZ; }
+// largest nvz the per-row tables in shared memory allow
+int tma_max_nvz() { return 1024; }
 
-template <int STAGE, class TC, class TIN, class TOUT>
+static const int TMA_SMEM_MAX = 232448;  // opt-in shared memory per block on sm_100
+
+template <int SCHEME, bool GEN, int STAGE, class TC, class TIN, class TOUT>
 static cudaError_t launch_one(const CUtensorMap &mX, const CUtensorMap &mY, const CUtensorMap &mA,
                               const StageArgs &a, int *err, int nblocks, cudaStream_t s)
 {
     using L = tma::Layout<TIN, STAGE>;
-    constexpr int NB = (L::BUF * 4 + 16 * 1024 <= 220 * 1024) ? 4 : 3;
-    const int shmem = NB * L::BUF + 2 * NB * 8 + (2 + tma::R) * NMOM * tma::TZ * 8;
-    auto kern = fd_stage_tma_kernel<STAGE, TC, TIN, TOUT, NB>;
-    if (nblocks <= 0) {  // preparation call: raise the dynamic shared-memory limit
-        return cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, shmem);
-    }
+    constexpr int FIXED = (2 + tma::R) * NMOM * tma::TZ * 8 + 2 * 1024 * 8 + 1024;
+    constexpr int NB = (L::BUF * 4 + FIXED <= TMA_SMEM_MAX) ? 4 : 3;
+    auto kern = rk4_stage_tma_kernel<SCHEME, GEN, STAGE, TC, TIN, TOUT, NB>;
+    if (nblocks <= 0)  // preparation call: raise the dynamic shared-memory limit
+        return cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, TMA_SMEM_MAX);
+    const int shmem = NB * L::BUF + 2 * NB * 8 + (2 + tma::R) * NMOM * tma::TZ * 8 + 2 * a.nvz * 8;
     kern<<<nblocks, tma::NTHR, shmem, s>>>(mX, mY, mA, a, err);
     return cudaGetLastError();
 }
 
-cudaError_t launch_fd_stage_tma(const CUtensorMap &mX, const CUtensorMap &mY,
-                                const CUtensorMap &mA, const StageArgs &a, int stage, int fp32,
-                                int *err, int nblocks, cudaStream_t s);
+template <int SCHEME, bool GEN>
+static cudaError_t launch_p(const CUtensorMap &mX, const CUtensorMap &mY, const CUtensorMap &mA,
+                            const StageArgs &a, int stage, int fp32, int *err, int nblocks,
+                            cudaStream_t s)
+{
+    if (fp32) {
+        switch (stage) {
+        case 1: return launch_one<SCHEME, GEN, 1, float, double, float>(mX, mY, mA, a, err, nblocks, s);
+        case 2: return launch_one<SCHEME, GEN, 2, float, float, float>(mX, mY, mA, a, err, nblocks, s);
+        case 3: return launch_one<SCHEME, GEN, 3, float, float, float>(mX, mY, mA, a, err, nblocks, s);
+        case 4: return launch_one<SCHEME, GEN, 4, float, float, double>(mX, mY, mA, a, err, nblocks, s);
+        }
+    } else {
+        switch (stage) {
+        case 1: return launch_one<SCHEME, GEN, 1, double, double, double>(mX, mY, mA, a, err, nblocks, s);
+        case 2: return launch_one<SCHEME, GEN, 2, double, double, double>(mX, mY, mA, a, err, nblocks, s);
+        case 3: return launch_one<SCHEME, GEN, 3, double, double, double>(mX, mY, mA, a, err, nblocks, s);
+        case 4: return launch_one<SCHEME, GEN, 4, double, double, double>(mX, mY, mA, a, err, nblocks, s);
+        }
+    }
+    return cudaErrorInvalidValue;
+}
+
+cudaError_t launch_rk4_stage_tma(const CUtensorMap &mX, const CUtensorMap &mY,
+                                 const CUtensorMap &mA, const StageArgs &a, int scheme, int stage,
+                                 int fp32, int *err, int nblocks, cudaStream_t s)
+{
+    if (scheme == FV) return launch_p<FV, false>(mX, mY, mA, a, stage, fp32, err, nblocks, s);
+    const bool gen = a.fd_advec != 0 || a.ko_order == 5;
+    return gen ? launch_p<FD, true>(mX, mY, mA, a, stage, fp32, err, nblocks, s)
+               : launch_p<FD, false>(mX, mY, mA, a, stage, fp32, err, nblocks, s);
+}
 
 // Sets the shared-memory attribute of every instantiation on the current device.
 cudaError_t tma_prepare()
 {
     CUtensorMap m{};
     StageArgs a{};
-    for (int fp32 = 0; fp32 < 2; ++fp32)
-        for (int st = 1; st <= 4; ++st) {
-            cudaError_t e = launch_fd_stage_tma(m, m, m, a, st, fp32, nullptr, 0, nullptr);
-            if (e != cudaSuccess) return e;
-        }
+    for (int sch = 0; sch < 2; ++sch)
+        for (int gen = 0; gen < 2; ++gen)
+            for (int fp32 = 0; fp32 < 2; ++fp32)
+                for (int st = 1; st <= 4; ++st) {
+                    a.fd_advec = gen;
+                    a.ko_order = 3;
+                    cudaError_t e = launch_rk4_stage_tma(m, m, m, a, sch, st, fp32, nullptr, 0, nullptr);
+                    if (e != cudaSuccess) return e;
+                }
     return cudaSuccess;
-}
-
-cudaError_t launch_fd_stage_tma(const CUtensorMap &mX, const CUtensorMap &mY,
-                                const CUtensorMap &mA, const StageArgs &a, int stage, int fp32,
-                                int *err, int nblocks, cudaStream_t s)
-{
-    if (fp32) {
-        switch (stage) {
-        case 1: return launch_one<1, float, double, float>(mX, mY, mA, a, err, nblocks, s);
-        case 2: return launch_one<2, float, float, float>(mX, mY, mA, a, err, nblocks, s);
-        case 3: return launch_one<3, float, float, float>(mX, mY, mA, a, err, nblocks, s);
-        case 4: return launch_one<4, float, float, double>(mX, mY, mA, a, err, nblocks, s);
-        }
-    } else {
-        switch (stage) {
-        case 1: return launch_one<1, double, double, double>(mX, mY, mA, a, err, nblocks, s);
-        case 2: return launch_one<2, double, double, double>(mX, mY, mA, a, err, nblocks, s);
-        case 3: return launch_one<3, double, double, double>(mX, mY, mA, a, err, nblocks, s);
-        case 4: return launch_one<4, double, double, double>(mX, mY, mA, a, err, nblocks, s);
-        }
-    }
-    return cudaErrorInvalidValue;
 }
 
 }  // namespace cosenu

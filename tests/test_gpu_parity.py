@@ -232,13 +232,15 @@ def test_errors_are_reported_not_fatal(gpu_lib, oracle):
 
 @pytest.mark.parametrize("precision", ["fp64", "fp32"])
 @pytest.mark.parametrize("bc", ["periodic", "open"])
-def test_fd_tma_path_equals_register_path(gpu_lib, oracle, precision, bc):
-    """The TMA-pipelined FD kernel (default for FD) and the register-tiled
-    kernel with the same 32 x nvz tile do the same arithmetic in the same
-    order: bitwise equal.  nvz = 37 leaves a partial 8-row chunk."""
+@pytest.mark.parametrize("scheme", ["fd", "fv"])
+def test_tma_path_equals_register_path(gpu_lib, oracle, scheme, precision, bc):
+    """The TMA-pipelined kernel (default when nz is a multiple of 32) and the
+    register-tiled kernel with the same 32 x nvz tile do the same arithmetic
+    in the same order: bitwise equal in FP64.  nvz = 37 leaves a partial
+    8-row chunk and puts rows of both signs of v in one chunk."""
     from oracle.oracle import Case
-    case = Case(nz=2048, nvz=37, gz=2, z0=-1024.0, z1=1024.0, scheme="fd", bc=bc, omega=1e-2,
-                theta_deg=37.0, mu=1.0)
+    case = Case(nz=2048, nvz=37, gz=4 if scheme == "fv" else 2, z0=-1024.0, z1=1024.0,
+                scheme=scheme, bc=bc, omega=1e-2, theta_deg=37.0, mu=1.0)
     outs = []
     for tiles in ({}, {"tile_z": 32, "tile_v": 37}):
         with gpu_from_case(case, precision=precision, **tiles) as sim:

@@ -139,8 +139,12 @@ void choose_tile(cosenu_ctx *ctx)
     const cosenu_params &p = ctx->p;
     const char *kenv = getenv("COSENU_KERNEL");
     bool force_ldg = kenv && std::string(kenv) == "ldg";
-    if (p.nz % 32 == 0 && p.nvz <= tma_max_nvz() && p.tile_z == 0 && p.tile_v == 0 && !force_ldg) {
-        // TMA path: 32-cell z tiles spanning all rows
+    bool force_tma = kenv && std::string(kenv) == "tma";
+    int nsm = 148;
+    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, p.device);
+    if (p.nz % 32 == 0 && (p.nz / 32 >= nsm || force_tma) && p.nvz <= tma_max_nvz() &&
+        p.tile_z == 0 && p.tile_v == 0 && !force_ldg) {
+        // TMA path (grids with at least one 32-cell z tile per SM): tiles span all rows
         ctx->use_tma = true;
         ctx->tz = 32;
         ctx->tv = p.nvz;

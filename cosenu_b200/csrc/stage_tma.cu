@@ -225,7 +225,7 @@ __global__ void __launch_bounds__(tma::NTHR, 1)
             const double *ys = reinterpret_cast<const double *>(buf + L::XB) + warp * TZ + lane;
             const double *as = reinterpret_cast<const double *>(buf + L::XB + L::YB) + warp * TZ + lane;
 
-            TC c[NCOMP], o[NCOMP];
+            TC c[NCOMP], o[NCOMP], ko[NCOMP];
             double x0[NCOMP];
 #pragma unroll
             for (int q = 0; q < NCOMP; ++q) {
@@ -303,22 +303,30 @@ __global__ void __launch_bounds__(tma::NTHR, 1)
                     o[BEXI] += hm * c[BEXR];
                 }
                 const int sv = (vzv > 0.0) - (vzv < 0.0);
+                // one pass over each stencil: advection now, dissipation kept
+                // for after the collective term (the reference's order)
 #pragma unroll
                 for (int q = 0; q < NCOMP; ++q) {
-                    if (!advec) continue;
                     const TIN *p = xs + q * (R * XW);
                     const TC m2 = (TC)p[-2], m1 = (TC)p[-1], p1 = (TC)p[1], p2 = (TC)p[2];
-                    TC adv;
-                    if (!GEN || a.fd_advec == 0) {
-                        adv = factor * ((m2 - p2) - TC(8) * (m1 - p1));
-                    } else if (a.fd_advec == 1) {
-                        adv = factor * (TC(-4) * (TC)p[-3 * sv] + TC(18) * (TC)p[-2 * sv] -
-                                        TC(36) * (TC)p[-sv] + TC(22) * c[q]);
-                    } else {
-                        adv = factor * ((TC)p[-3 * sv] - TC(6) * (TC)p[-2 * sv] +
-                                        TC(18) * (TC)p[-sv] - TC(10) * c[q] - TC(3) * (TC)p[sv]);
+                    if (advec) {
+                        TC adv;
+                        if (!GEN || a.fd_advec == 0) {
+                            adv = factor * ((m2 - p2) - TC(8) * (m1 - p1));
+                        } else if (a.fd_advec == 1) {
+                            adv = factor * (TC(-4) * (TC)p[-3 * sv] + TC(18) * (TC)p[-2 * sv] -
+                                            TC(36) * (TC)p[-sv] + TC(22) * c[q]);
+                        } else {
+                            adv = factor * ((TC)p[-3 * sv] - TC(6) * (TC)p[-2 * sv] +
+                                            TC(18) * (TC)p[-sv] - TC(10) * c[q] - TC(3) * (TC)p[sv]);
+                        }
+                        o[q] += adv;
                     }
-                    o[q] += adv;
+                    if (GEN && a.ko_order == 5)
+                        ko[q] = ko_eps * ((TC)p[-3] + (TC)p[3] - TC(6) * (m2 + p2) +
+                                          TC(15) * (m1 + p1) - TC(20) * c[q]);
+                    else
+                        ko[q] = ko_eps * (m2 + p2 - TC(4) * (m1 + p1) + TC(6) * c[q]);
                 }
             }
             if (coll) {
@@ -337,17 +345,7 @@ __global__ void __launch_bounds__(tma::NTHR, 1)
             }
             if (SCHEME == FD) {
 #pragma unroll
-                for (int q = 0; q < NCOMP; ++q) {
-                    const TIN *p = xs + q * (R * XW);
-                    const TC m2 = (TC)p[-2], m1 = (TC)p[-1], p1 = (TC)p[1], p2 = (TC)p[2];
-                    TC ko;
-                    if (GEN && a.ko_order == 5)
-                        ko = ko_eps * ((TC)p[-3] + (TC)p[3] - TC(6) * (m2 + p2) + TC(15) * (m1 + p1) -
-                                       TC(20) * c[q]);
-                    else
-                        ko = ko_eps * (m2 + p2 - TC(4) * (m1 + p1) + TC(6) * c[q]);
-                    o[q] += ko;
-                }
+                for (int q = 0; q < NCOMP; ++q) o[q] += ko[q];
             }
 
             // stage combine

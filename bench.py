@@ -384,6 +384,76 @@ def run_reference_arm(args):
     }), flush=True)
 
 
+def run_ensemble(args):
+    """256 uneven FV instances to t = 1000/mu in one ensemble
+    (autotuned kernel family and tiles), against the plain single-instance
+    FP64 path timed on a stratified subset (every 8th instance, full step
+    counts) and scaled by work."""
+    import torch
+
+    from cosenu_b200 import NuOsc
+    from cosenu_b200.ensemble import Ensemble, ensemble_instances
+
+    torch.cuda.set_device(0)
+    stream = torch.cuda.Stream()
+    torch.cuda.set_stream(stream)
+    xs = ensemble_instances(args.instances, t_factor=args.t_factor)
+    work = [x.cells * x.nsteps for x in xs]
+    ens = Ensemble(xs, precision=args.precision)
+    ens.set_stream(stream.cuda_stream)
+    ens.init_seeded()
+    report = ens.autotune(trial_steps=3)
+    cfg = ens.config()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(0) as clk:
+        torch.cuda.synchronize()
+        ev0.record(stream)
+        ens.run()
+        ev1.record(stream)
+        ens.synchronize()
+        torch.cuda.synchronize()
+    t_batch = ev0.elapsed_time(ev1) / 1e3
+    pee = [m.analyse()["Pee"] for m in ens.members]
+    ens.close()
+    # plain path: every 8th instance alone, FP64, default kernel choice
+    sub = list(range(0, len(xs), 8))
+    t_sub = 0.0
+    for i in sub:
+        x = xs[i]
+        sim = NuOsc(nz=x.nz, nvz=x.nvz, gz=4, z0=x.z0, z1=x.z1, cfl=x.cfl, omega=0.0, mu=x.mu,
+                    scheme="fv")
+        sim.set_stream(stream.cuda_stream)
+        sim.init_seeded(x.seed, instance=i, sig_nu=x.sig_nu, sig_nubar=x.sig_nubar,
+                        alpha=x.alpha)
+        torch.cuda.synchronize()
+        ev0.record(stream)
+        sim.evolve(x.nsteps)
+        ev1.record(stream)
+        torch.cuda.synchronize()
+        t_sub += ev0.elapsed_time(ev1) / 1e3
+        if args.precision == "fp64":
+            d = abs(sim.analyse()["Pee"] - pee[i])
+            if d > 1e-9:
+                raise SystemExit(f"ensemble member {i} differs from the plain path: {d}")
+        sim.close()
+    w_sub = sum(work[i] for i in sub)
+    t_plain = t_sub * sum(work) / w_sub
+    n = len(xs)
+    print(json.dumps({
+        "metric": "instances/s (configs[3] ensemble to t = 1000/mu)", "value": n / t_batch,
+        "unit": "instances/s", "n_gpus": 1, "instances": n,
+        "cell_updates_per_s": sum(work) / t_batch, "seconds": t_batch,
+        "plain_fp64_instances_per_s": n / t_plain,
+        "plain_fp64_note": f"{len(sub)} of {n} instances run alone ({t_sub:.1f} s), scaled by work",
+        "speedup_vs_plain": t_plain / t_batch, "higher_is_better": True,
+        "precision": args.precision.upper(), "data": "synthetic",
+        "config": {"workload": "256 FV WENO7 instances, nz logU[512,8192]/256, nvz {32..256}, "
+                               "alpha U[.6,1.2], sigma U[.4,.8]/U[.3,.7], mu U[.5,2], "
+                               "t = 1000/mu", "kernel": cfg, "t_factor": args.t_factor},
+        "autotune": report.strip().splitlines(), "clocks": clk.summary(),
+    }), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -391,7 +461,9 @@ def main():
     ap.add_argument("--warmup", type=int, default=10)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--workload", choices=sorted(WORKLOADS), default="c2",
+    ap.add_argument("--instances", type=int, default=256, help="c4: ensemble size")
+    ap.add_argument("--t-factor", type=float, default=1000.0, help="c4: run to t_factor/mu")
+    ap.add_argument("--workload", choices=sorted(WORKLOADS) + ["c4"], default="c2",
                     help="c2 (default, the headline): FD 32768 x 256; c1: FV 1024 x 64; "
                          "c3: FV 65536 x 512")
     ap.add_argument("--precision", choices=["fp64", "fp32"], default="fp64")
@@ -399,6 +471,9 @@ def main():
                     help="smaller z extent at the same dz (profiling cases only; the headline "
                          "workload is nz = 32768)")
     args = ap.parse_args()
+    if args.workload == "c4":
+        run_ensemble(args)
+        return
     WORKLOAD.clear()
     WORKLOAD.update(WORKLOADS[args.workload])
     if args.nz is None:

@@ -28,6 +28,10 @@ EXPORTS = (
     "cosenu_init_reference", "cosenu_device_state", "cosenu_upload_device",
     "cosenu_download_device", "cosenu_launches_per_step", "cosenu_tile", "cosenu_device_bytes",
     "cosenu_step_noalloc",
+    "cosenu_batch_create", "cosenu_batch_destroy", "cosenu_batch_last_error",
+    "cosenu_batch_size", "cosenu_batch_member", "cosenu_batch_init_seeded", "cosenu_batch_run",
+    "cosenu_batch_synchronize", "cosenu_batch_autotune", "cosenu_batch_config",
+    "cosenu_batch_set_config", "cosenu_batch_set_stream",
 )
 
 
@@ -100,6 +104,18 @@ def load(path: str | None = None) -> C.CDLL:
         "cosenu_tile": (i, [vp, C.POINTER(i), C.POINTER(i)]),
         "cosenu_device_bytes": (i, [vp, C.POINTER(C.c_size_t)]),
         "cosenu_step_noalloc": (i, [C.POINTER(Params), DPTR8, i, i, vp]),
+        "cosenu_batch_create": (i, [i, C.POINTER(Params), C.POINTER(vp)]),
+        "cosenu_batch_destroy": (i, [vp]),
+        "cosenu_batch_last_error": (C.c_char_p, [vp]),
+        "cosenu_batch_size": (i, [vp]),
+        "cosenu_batch_member": (vp, [vp, i]),
+        "cosenu_batch_init_seeded": (i, [vp, vp, vp, vp, vp, d]),
+        "cosenu_batch_run": (i, [vp, vp]),
+        "cosenu_batch_synchronize": (i, [vp]),
+        "cosenu_batch_autotune": (i, [vp, i, C.c_char_p, C.c_size_t]),
+        "cosenu_batch_config": (i, [vp, C.POINTER(i), C.POINTER(i), vp]),
+        "cosenu_batch_set_config": (i, [vp, i, i, vp]),
+        "cosenu_batch_set_stream": (i, [vp, vp]),
     }
     for name, (res, args) in sig.items():
         f = getattr(lib, name)

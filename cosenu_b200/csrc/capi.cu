@@ -8,18 +8,9 @@
 #include <string>
 #include <vector>
 
-#include <cuda.h>
-
-#include "../../include/cosenu_b200.h"
-#include "common.cuh"
+#include "ctx.h"
 
 namespace cosenu {
-cudaError_t launch_rk4_stage(const StageArgs &a, int scheme, int stage, int tz, int fp32,
-                             cudaStream_t s);
-cudaError_t launch_ghost_fill(double *buf, long long cs, int ld, int nz, int nvz, int H, int bc,
-                              cudaStream_t s);
-cudaError_t launch_moments(const double *X, double *M, const double *vz, long long cs, int ld,
-                           int nz, int nvz, int tz, int tv, cudaStream_t s);
 int diag_blocks();
 int diag_slots();
 cudaError_t launch_diag(const double *Y, const double *S0, const double *G, const double *bG,
@@ -33,53 +24,12 @@ cudaError_t launch_init_seeded(double *Y, double *G, double *bG, const double *G
 cudaError_t launch_init_reference(double *Y, double *G, double *bG, const double *Gv,
                                   const double *bGv, const double *ez, const double *ez_,
                                   long long cs, int ld, int nz, int nvz, cudaStream_t s);
-int make_state_map(CUtensorMap *map, const void *base, int elem_bytes, int ld, int nvz,
-                   long long cs, int box_cells);
-int tma_box_x();
-int tma_box_tile();
-cudaError_t tma_prepare();
-int tma_max_nvz();
-cudaError_t launch_rk4_stage_tma(const CUtensorMap &mX, const CUtensorMap &mY,
-                                 const CUtensorMap &mA, const StageArgs &a, int scheme, int stage,
-                                 int fp32, int *err, int nblocks, cudaStream_t s);
 }  // namespace cosenu
 
 using namespace cosenu;
 
 // message for cosenu_last_error(NULL): failures that have no context
 thread_local std::string g_create_error;
-
-struct cosenu_ctx {
-    cosenu_params p{};
-    int ld = 0, H = 4, tz = 32, tv = 64, nvt = 1;
-    long long cs = 0;
-    double dz = 0, dv = 0, dt = 0, ct = 0, st = 0;
-    int fp32 = 0;
-    cudaStream_t own_stream = nullptr, stream = nullptr;
-    // device memory
-    double *Y = nullptr, *A = nullptr, *S0 = nullptr, *G = nullptr, *bG = nullptr;
-    void *U0 = nullptr, *U1 = nullptr;
-    double *M[3] = {nullptr, nullptr, nullptr};
-    double *vz = nullptr, *rowfac = nullptr, *Hm = nullptr;
-    double *diag_part = nullptr, *diag_out = nullptr, *pee = nullptr, *tmp = nullptr;
-    size_t bytes = 0;
-    // host mirrors
-    std::vector<double> h_vz, h_rowfac, h_Hm, h_Z;
-    double *h_pinned = nullptr;  // small pinned buffer for results
-    // TMA-pipelined FD path: tensor maps over Y, U0, U1 (input boxes) and Y, A
-    bool use_tma = false;
-    int nsm = 148;
-    CUtensorMap mY40, mU0_40, mU1_40, mY32, mA32;
-    int *err_flag = nullptr;  // device word set by bounded waits that expired
-    // graphs of 1 and GRAPH_CHUNK steps
-    cudaGraphExec_t g1 = nullptr, gN = nullptr;
-    bool use_graphs = true;
-    // status
-    bool have_state = false, have_profile = false, have_state0 = false;
-    int next_stage = 0;
-    long long steps = 0;
-    std::string err;
-};
 
 static const int GRAPH_CHUNK = 16;
 
@@ -134,7 +84,7 @@ int alloc(cosenu_ctx *ctx, void **p, size_t n)
     return COSENU_OK;
 }
 
-void choose_tile(cosenu_ctx *ctx)
+void choose_tile(cosenu_ctx *ctx, int layout = 0)
 {
     const cosenu_params &p = ctx->p;
     const char *kenv = getenv("COSENU_KERNEL");
@@ -142,8 +92,9 @@ void choose_tile(cosenu_ctx *ctx)
     bool force_tma = kenv && std::string(kenv) == "tma";
     int nsm = 148;
     cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, p.device);
-    if (p.nz % 32 == 0 && (p.nz / 32 >= nsm || force_tma) && p.nvz <= tma_max_nvz() &&
-        p.tile_z == 0 && p.tile_v == 0 && !force_ldg) {
+    if (p.nz % 32 == 0 && p.nvz <= tma_max_nvz() &&
+        (layout == 1 || ((p.nz / 32 >= nsm || force_tma) && p.tile_z == 0 && p.tile_v == 0 &&
+                         !force_ldg))) {
         // TMA path (grids with at least one 32-cell z tile per SM): tiles span all rows
         ctx->use_tma = true;
         ctx->tz = 32;
@@ -322,7 +273,11 @@ const char *cosenu_last_error(const cosenu_ctx *ctx)
     return ctx ? ctx->err.c_str() : g_create_error.c_str();
 }
 
-int cosenu_create(const cosenu_params *pp, cosenu_ctx **out)
+int cosenu_create(const cosenu_params *pp, cosenu_ctx **out) { return ctx_create(pp, out, 0); }
+
+}  // extern "C"
+
+int ctx_create(const cosenu_params *pp, cosenu_ctx **out, int layout)
 {
     g_create_error.clear();
     if (!pp || !out) {
@@ -364,7 +319,12 @@ int cosenu_create(const cosenu_params *pp, cosenu_ctx **out)
     ctx->ld = padded_ld(p.nz);
     ctx->cs = (long long)p.nvz * ctx->ld;
     ctx->H = std::max(4, p.gz);
-    choose_tile(ctx);
+    choose_tile(ctx, layout);
+    if (layout == 1 && !ctx->use_tma) {
+        g_create_error = "ensemble members need nz % 32 == 0 and nvz <= 1024";
+        delete ctx;
+        return COSENU_ERR_ARG;
+    }
     // grid exactly as NuOsc::NuOsc and set_vac_pars (src/nuosc.hpp:78-96,132-138)
     ctx->dz = (p.z1 - p.z0) / p.nz;
     ctx->dv = (p.v1 - p.v0) / (p.nvz);
@@ -396,7 +356,9 @@ int cosenu_create(const cosenu_params *pp, cosenu_ctx **out)
     const size_t plane = (size_t)ctx->cs * sizeof(double);
     const size_t state = plane * NCOMP;
     const size_t ustate = ctx->fp32 ? state / 2 : state;
-    const size_t mom = (size_t)ctx->nvt * NMOM * p.nz * sizeof(double);
+    // ensemble members may later be re-tiled down to 8-row v tiles
+    ctx->mom_nvt_cap = layout == 1 ? (p.nvz + 7) / 8 : ctx->nvt;
+    const size_t mom = (size_t)ctx->mom_nvt_cap * NMOM * p.nz * sizeof(double);
 #define AL(ptr, n)                                                              \
     if ((rc = alloc(ctx, (void **)&(ptr), (n))) != COSENU_OK) {                 \
         g_create_error = ctx->err;                                              \
@@ -469,6 +431,31 @@ int cosenu_create(const cosenu_params *pp, cosenu_ctx **out)
     *out = ctx;
     return COSENU_OK;
 }
+
+StageArgs ctx_stage_args(const cosenu_ctx *ctx, int stage) { return stage_args(ctx, stage); }
+int ctx_prepare_state(cosenu_ctx *ctx) { return prepare_state(ctx); }
+
+int ctx_set_tiling(cosenu_ctx *ctx, int tz, int tv)
+{
+    if (tz == 0) {
+        ctx->tz = 32;
+        ctx->tv = ctx->p.nvz;
+        ctx->nvt = 1;
+        ctx->use_tma = true;
+    } else {
+        int nvt = (ctx->p.nvz + tv - 1) / tv;
+        if (ctx->p.nz % tz != 0 || nvt > ctx->mom_nvt_cap || tv > MAX_TV)
+            return fail(ctx, COSENU_ERR_ARG, "tile does not fit this member");
+        ctx->tz = tz;
+        ctx->tv = tv;
+        ctx->nvt = nvt;
+        ctx->use_tma = false;
+    }
+    drop_graphs(ctx);
+    return ctx->have_state ? prepare_state(ctx) : COSENU_OK;
+}
+
+extern "C" {
 
 int cosenu_destroy(cosenu_ctx *ctx)
 {

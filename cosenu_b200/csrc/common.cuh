@@ -10,6 +10,7 @@
 // aligned ghost zone.
 #pragma once
 
+#include <cuda.h>
 #include <cuda_runtime.h>
 #include <stdint.h>
 
@@ -41,6 +42,17 @@ struct StageArgs {
     int H;               // ghost cells written per side
     int bc, flags, fd_advec, ko_order;
     double dt, dv, mu, ct, st, pmo, ko_eps;
+};
+
+// Ensemble launch: one stage launch covers every active instance.  Entry t of
+// `table` names (instance, z tile, v tile); `args` holds the four stage
+// arguments of every instance and `maps` its five tensor maps (Y and U0/U1
+// input boxes, Y and A tile boxes).
+struct BatchDev {
+    const int4 *table;
+    int ntiles;
+    const StageArgs *args;      // [instances][4]
+    const CUtensorMap *maps;    // [instances][5]
 };
 
 // Layout helpers shared by host and device code.

@@ -1,0 +1,81 @@
+// Internal definitions shared by the C-ABI translation units (context layout,
+// launchers).  Not part of the public interface.
+#pragma once
+
+#include <cuda.h>
+
+#include <string>
+#include <vector>
+
+#include "../../include/cosenu_b200.h"
+#include "common.cuh"
+
+namespace cosenu {
+cudaError_t launch_rk4_stage(const StageArgs &a, int scheme, int stage, int tz, int fp32,
+                             cudaStream_t s);
+cudaError_t launch_ghost_fill(double *buf, long long cs, int ld, int nz, int nvz, int H, int bc,
+                              cudaStream_t s);
+cudaError_t launch_moments(const double *X, double *M, const double *vz, long long cs, int ld,
+                           int nz, int nvz, int tz, int tv, cudaStream_t s);
+int make_state_map(CUtensorMap *map, const void *base, int elem_bytes, int ld, int nvz,
+                   long long cs, int box_cells);
+int tma_box_x();
+int tma_box_tile();
+int tma_max_nvz();
+cudaError_t tma_prepare();
+cudaError_t launch_rk4_stage_tma(const CUtensorMap &mX, const CUtensorMap &mY,
+                                 const CUtensorMap &mA, const StageArgs &a, int scheme, int stage,
+                                 int fp32, int *err, int nblocks, cudaStream_t s);
+cudaError_t launch_rk4_stage_tma_batch(const BatchDev &bd, const StageArgs &a, int scheme,
+                                       int stage, int fp32, int *err, int nblocks, int max_nvz,
+                                       cudaStream_t s);
+cudaError_t launch_rk4_stage_batch(const BatchDev &bd, int scheme, int stage, int tz, int fp32,
+                                   cudaStream_t s);
+}  // namespace cosenu
+
+// One simulation on one GPU.
+struct cosenu_ctx {
+    cosenu_params p{};
+    int ld = 0, H = 4, tz = 32, tv = 64, nvt = 1;
+    long long cs = 0;
+    double dz = 0, dv = 0, dt = 0, ct = 0, st = 0;
+    int fp32 = 0;
+    cudaStream_t own_stream = nullptr, stream = nullptr;
+    // device memory
+    double *Y = nullptr, *A = nullptr, *S0 = nullptr, *G = nullptr, *bG = nullptr;
+    void *U0 = nullptr, *U1 = nullptr;
+    double *M[3] = {nullptr, nullptr, nullptr};
+    double *vz = nullptr, *rowfac = nullptr, *Hm = nullptr;
+    double *diag_part = nullptr, *diag_out = nullptr, *pee = nullptr, *tmp = nullptr;
+    size_t bytes = 0;
+    // host mirrors
+    std::vector<double> h_vz, h_rowfac, h_Hm, h_Z;
+    double *h_pinned = nullptr;  // small pinned buffer for results
+    // TMA-pipelined FD path: tensor maps over Y, U0, U1 (input boxes) and Y, A
+    bool use_tma = false;
+    int nsm = 148;
+    CUtensorMap mY40, mU0_40, mU1_40, mY32, mA32;
+    int *err_flag = nullptr;  // device word set by bounded waits that expired
+    // graphs of 1 and GRAPH_CHUNK steps
+    cudaGraphExec_t g1 = nullptr, gN = nullptr;
+    bool use_graphs = true;
+    // status
+    bool have_state = false, have_profile = false, have_state0 = false;
+    int next_stage = 0;
+    long long steps = 0;
+    int mom_nvt_cap = 1;  // v tiles the moment buffers have room for
+    std::string err;
+};
+
+
+// Context creation; layout 1 forces the TMA layout (32-cell z tiles spanning
+// all rows, tensor maps built) whatever the grid size, as ensemble members
+// need it.
+int ctx_create(const cosenu_params *p, cosenu_ctx **out, int layout);
+// Arguments of stage 1..4 of a context.
+cosenu::StageArgs ctx_stage_args(const cosenu_ctx *ctx, int stage);
+// Ghost cells and input moments of Y after Y changed outside the stages.
+int ctx_prepare_state(cosenu_ctx *ctx);
+// Re-tiles an ensemble member for the register-tiled kernel (tz x tv) or back
+// to the TMA layout (tz = 0); recomputes the input moments of Y.
+int ctx_set_tiling(cosenu_ctx *ctx, int tz, int tv);

@@ -83,9 +83,20 @@ __device__ __forceinline__ void fd_terms(const TIN *__restrict__ p, int fd_advec
 }
 
 // ---------------------------------------------------------------------------
-template <int SCHEME, int STAGE, int TZ, class TC, class TIN, class TOUT>
-__global__ void __launch_bounds__(NTHREADS, 2) rk4_stage_kernel(const StageArgs a)
+template <int SCHEME, int STAGE, int TZ, class TC, class TIN, class TOUT, bool BATCHED>
+__global__ void __launch_bounds__(NTHREADS, 2)
+    rk4_stage_kernel(const __grid_constant__ StageArgs a0, const BatchDev bd)
 {
+    // tile: (z tile, v tile) from the grid, or (instance, z tile, v tile) from
+    // the ensemble table
+    int zt = blockIdx.x, vt = blockIdx.y, inst = 0;
+    if (BATCHED) {
+        const int4 e = bd.table[blockIdx.x];
+        inst = e.x;
+        zt = e.y;
+        vt = e.z;
+    }
+    const StageArgs &a = BATCHED ? bd.args[inst * 4 + STAGE - 1] : a0;
     constexpr int RP = NTHREADS / TZ;
     __shared__ double s_mom[NMOM][TZ];
     __shared__ double s_red[RP][NMOM][TZ];
@@ -96,9 +107,8 @@ __global__ void __launch_bounds__(NTHREADS, 2) rk4_stage_kernel(const StageArgs 
     const int tid = threadIdx.x;
     const int lz = tid % TZ;
     const int rr = tid / TZ;
-    const int z0 = blockIdx.x * TZ;
+    const int z0 = zt * TZ;
     const int z = z0 + lz;
-    const int vt = blockIdx.y;
     const int vbeg = vt * a.tv;
     const int vend = min(vbeg + a.tv, a.nvz);
     const int nrows = vend - vbeg;
@@ -346,44 +356,62 @@ __global__ void __launch_bounds__(NTHREADS, 2) rk4_stage_kernel(const StageArgs 
 // ---------------------------------------------------------------------------
 // host launcher
 
-template <int SCHEME, int TZ, class TC, class TIN1, class TU>
-static cudaError_t launch_t(const StageArgs &a, int stage, cudaStream_t s)
+template <int SCHEME, int TZ, class TC, class TIN1, class TU, bool B>
+static cudaError_t launch_t(const StageArgs &a, int stage, cudaStream_t s, const BatchDev &bd)
 {
-    dim3 grid(a.nz / TZ, a.nvt), block(NTHREADS);
+    dim3 grid = B ? dim3(bd.ntiles) : dim3(a.nz / TZ, a.nvt), block(NTHREADS);
+    if (grid.x == 0) return cudaSuccess;
     switch (stage) {
-    case 1: rk4_stage_kernel<SCHEME, 1, TZ, TC, TIN1, TU><<<grid, block, 0, s>>>(a); break;
-    case 2: rk4_stage_kernel<SCHEME, 2, TZ, TC, TU, TU><<<grid, block, 0, s>>>(a); break;
-    case 3: rk4_stage_kernel<SCHEME, 3, TZ, TC, TU, TU><<<grid, block, 0, s>>>(a); break;
-    case 4: rk4_stage_kernel<SCHEME, 4, TZ, TC, TU, double><<<grid, block, 0, s>>>(a); break;
+    case 1: rk4_stage_kernel<SCHEME, 1, TZ, TC, TIN1, TU, B><<<grid, block, 0, s>>>(a, bd); break;
+    case 2: rk4_stage_kernel<SCHEME, 2, TZ, TC, TU, TU, B><<<grid, block, 0, s>>>(a, bd); break;
+    case 3: rk4_stage_kernel<SCHEME, 3, TZ, TC, TU, TU, B><<<grid, block, 0, s>>>(a, bd); break;
+    case 4: rk4_stage_kernel<SCHEME, 4, TZ, TC, TU, double, B><<<grid, block, 0, s>>>(a, bd); break;
     default: return cudaErrorInvalidValue;
     }
     return cudaGetLastError();
 }
 
-template <int SCHEME, int TZ>
-static cudaError_t launch_p(const StageArgs &a, int stage, int fp32, cudaStream_t s)
+template <int SCHEME, int TZ, bool B>
+static cudaError_t launch_p(const StageArgs &a, int stage, int fp32, cudaStream_t s,
+                            const BatchDev &bd)
 {
-    return fp32 ? launch_t<SCHEME, TZ, float, double, float>(a, stage, s)
-                : launch_t<SCHEME, TZ, double, double, double>(a, stage, s);
+    return fp32 ? launch_t<SCHEME, TZ, float, double, float, B>(a, stage, s, bd)
+                : launch_t<SCHEME, TZ, double, double, double, B>(a, stage, s, bd);
+}
+
+template <bool B>
+static cudaError_t launch_s(const StageArgs &a, int scheme, int stage, int tz, int fp32,
+                            cudaStream_t s, const BatchDev &bd)
+{
+    if (scheme == FV) {
+        switch (tz) {
+        case 8: return launch_p<FV, 8, B>(a, stage, fp32, s, bd);
+        case 16: return launch_p<FV, 16, B>(a, stage, fp32, s, bd);
+        case 32: return launch_p<FV, 32, B>(a, stage, fp32, s, bd);
+        }
+    } else {
+        switch (tz) {
+        case 8: return launch_p<FD, 8, B>(a, stage, fp32, s, bd);
+        case 16: return launch_p<FD, 16, B>(a, stage, fp32, s, bd);
+        case 32: return launch_p<FD, 32, B>(a, stage, fp32, s, bd);
+        }
+    }
+    return cudaErrorInvalidValue;
 }
 
 cudaError_t launch_rk4_stage(const StageArgs &a, int scheme, int stage, int tz, int fp32,
                              cudaStream_t s)
 {
-    if (scheme == FV) {
-        switch (tz) {
-        case 8: return launch_p<FV, 8>(a, stage, fp32, s);
-        case 16: return launch_p<FV, 16>(a, stage, fp32, s);
-        case 32: return launch_p<FV, 32>(a, stage, fp32, s);
-        }
-    } else {
-        switch (tz) {
-        case 8: return launch_p<FD, 8>(a, stage, fp32, s);
-        case 16: return launch_p<FD, 16>(a, stage, fp32, s);
-        case 32: return launch_p<FD, 32>(a, stage, fp32, s);
-        }
-    }
-    return cudaErrorInvalidValue;
+    return launch_s<false>(a, scheme, stage, tz, fp32, s, BatchDev{});
+}
+
+// Ensemble launch: one block per table entry (instance, z tile, v tile); the
+// z tile width tz is shared by the launch, the v tile is per instance.
+cudaError_t launch_rk4_stage_batch(const BatchDev &bd, int scheme, int stage, int tz, int fp32,
+                                   cudaStream_t s)
+{
+    StageArgs a{};
+    return launch_s<true>(a, scheme, stage, tz, fp32, s, bd);
 }
 
 }  // namespace cosenu

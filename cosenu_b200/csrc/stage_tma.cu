@@ -39,6 +39,7 @@ constexpr int R = 8;             // rows per chunk = consumer warps
 constexpr int NCONS = R * 32;    // consumer threads
 constexpr int NTHR = NCONS + 32; // + producer warp
 constexpr unsigned long long WAIT_NS = 2000000000ull;  // 2 s per wait
+#define TMA_MAX_NVZ 1024
 
 __device__ __forceinline__ uint32_t smem_u32(const void *p)
 {
@@ -125,11 +126,25 @@ template <class TIN, int STAGE> struct Layout {
 
 }  // namespace tma
 
-template <int SCHEME, bool GEN, int STAGE, class TC, class TIN, class TOUT, int NBUF>
+template <bool BATCHED>
+__device__ __forceinline__ void tma_tile(const BatchDev &bd, int t, int &inst, int &zt)
+{
+    if (BATCHED) {
+        const int4 e = bd.table[t];
+        inst = e.x;
+        zt = e.y;
+    } else {
+        inst = 0;
+        zt = t;
+    }
+}
+
+template <int SCHEME, bool GEN, int STAGE, class TC, class TIN, class TOUT, int NBUF, bool BATCHED>
 __global__ void __launch_bounds__(tma::NTHR, 1)
     rk4_stage_tma_kernel(const __grid_constant__ CUtensorMap mX,
                          const __grid_constant__ CUtensorMap mY,
-                         const __grid_constant__ CUtensorMap mA, const StageArgs a, int *err)
+                         const __grid_constant__ CUtensorMap mA,
+                         const __grid_constant__ StageArgs a0, int *err, const BatchDev bd)
 {
     using namespace tma;
     using L = Layout<TIN, STAGE>;
@@ -139,14 +154,10 @@ __global__ void __launch_bounds__(tma::NTHR, 1)
     double(*s_mom)[NMOM][TZ] = reinterpret_cast<double(*)[NMOM][TZ]>(empty + NBUF);
     double(*s_red)[NMOM][TZ] = s_mom + 2;
     double *s_vz = reinterpret_cast<double *>(s_red + R);  // [nvz] velocities
-    double *s_fac = s_vz + a.nvz;                          // [nvz] advection factors
+    double *s_fac = s_vz + TMA_MAX_NVZ;                    // [nvz] advection factors
 
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-    const int nzt = a.nz / TZ;
-    const int nch = (a.nvz + R - 1) / R;
-    const bool coll = (a.flags & F_COLL) != 0;
-    const bool advec = (a.flags & F_ADVEC_OFF) == 0;
-    const bool open_bc = a.bc != 0;
+    const int nzt = BATCHED ? bd.ntiles : a0.nz / TZ;
 
     if (tid == 0) {
         for (int b = 0; b < NBUF; ++b) {
@@ -162,17 +173,25 @@ __global__ void __launch_bounds__(tma::NTHR, 1)
         if (lane == 0) {
             uint32_t it = 0;
             for (int t = blockIdx.x; t < nzt; t += gridDim.x) {
-                const int z0 = t * TZ;
+                int inst, zt;
+                tma_tile<BATCHED>(bd, t, inst, zt);
+                const StageArgs &a = BATCHED ? bd.args[inst * 4 + STAGE - 1] : a0;
+                const CUtensorMap *px =
+                    BATCHED ? &bd.maps[inst * 5 + (STAGE == 1 ? 0 : (STAGE == 3 ? 2 : 1))] : &mX;
+                const CUtensorMap *py = BATCHED ? &bd.maps[inst * 5 + 3] : &mY;
+                const CUtensorMap *pa = BATCHED ? &bd.maps[inst * 5 + 4] : &mA;
+                const int z0 = zt * TZ;
+                const int nch = (a.nvz + R - 1) / R;
                 for (int ch = 0; ch < nch; ++ch, ++it) {
                     const int b = it % NBUF;
                     if (it >= (uint32_t)NBUF)
                         tma::mbar_wait(&empty[b], ((it / NBUF) - 1) & 1, err, 1);
                     unsigned char *buf = smem + b * L::BUF;
                     tma::mbar_expect_tx(&full[b], L::XB + L::YB + L::AB);
-                    tma::tma_load_3d(buf, &mX, HP + z0 - HALO, ch * R, 0, &full[b]);
-                    if (L::YB) tma::tma_load_3d(buf + L::XB, &mY, HP + z0, ch * R, 0, &full[b]);
+                    tma::tma_load_3d(buf, px, HP + z0 - HALO, ch * R, 0, &full[b]);
+                    if (L::YB) tma::tma_load_3d(buf + L::XB, py, HP + z0, ch * R, 0, &full[b]);
                     if (L::AB)
-                        tma::tma_load_3d(buf + L::XB + L::YB, &mA, HP + z0, ch * R, 0, &full[b]);
+                        tma::tma_load_3d(buf + L::XB + L::YB, pa, HP + z0, ch * R, 0, &full[b]);
                 }
             }
         }
@@ -180,31 +199,58 @@ __global__ void __launch_bounds__(tma::NTHR, 1)
     }
 
     // ---------------------------------------------------------------- consumers
-    const double dt = a.dt;
-    const TC pmo = (TC)a.pmo, ct = (TC)a.ct, st = (TC)a.st, mudv = (TC)(a.mu * a.dv);
-    const TC ko_eps = (TC)a.ko_eps;
-    for (int i = tid; i < a.nvz; i += NCONS) {
-        s_vz[i] = a.vz[i];
-        s_fac[i] = a.rowfac[i];
-    }
+    if (!BATCHED)
+        for (int i = tid; i < a0.nvz; i += NCONS) {
+            s_vz[i] = a0.vz[i];
+            s_fac[i] = a0.rowfac[i];
+        }
     // moments of the stage input for the first tile
     int k = 0;
-    if (coll && tid < NMOM * TZ && (int)blockIdx.x < nzt) {
-        const int m = tid / TZ, zz = tid % TZ;
-        s_mom[0][m][zz] = a.Min[(long long)m * a.nz + blockIdx.x * TZ + zz];
+    if ((int)blockIdx.x < nzt && tid < NMOM * TZ) {
+        int inst, zt;
+        tma_tile<BATCHED>(bd, blockIdx.x, inst, zt);
+        const StageArgs &a = BATCHED ? bd.args[inst * 4 + STAGE - 1] : a0;
+        if (a.flags & F_COLL)
+            s_mom[0][tid / TZ][tid % TZ] = a.Min[(long long)(tid / TZ) * a.nz + zt * TZ + tid % TZ];
     }
     consumer_sync();
 
     uint32_t it = 0;
+    int prev_inst = -1;
     for (int t = blockIdx.x; t < nzt; t += gridDim.x, ++k) {
-        const int z0 = t * TZ;
+        int inst, zt;
+        tma_tile<BATCHED>(bd, t, inst, zt);
+        const StageArgs &a = BATCHED ? bd.args[inst * 4 + STAGE - 1] : a0;
+        if (BATCHED && inst != prev_inst) {
+            // per-row tables of this instance
+            consumer_sync();
+            for (int i = tid; i < a.nvz; i += NCONS) {
+                s_vz[i] = a.vz[i];
+                s_fac[i] = a.rowfac[i];
+            }
+            consumer_sync();
+            prev_inst = inst;
+        }
+        const int nch = (a.nvz + R - 1) / R;
+        const bool coll = (a.flags & F_COLL) != 0;
+        const bool advec = (a.flags & F_ADVEC_OFF) == 0;
+        const bool open_bc = a.bc != 0;
+        const double dt = a.dt;
+        const TC pmo = (TC)a.pmo, ct = (TC)a.ct, st = (TC)a.st, mudv = (TC)(a.mu * a.dv);
+        const TC ko_eps = (TC)a.ko_eps;
+        const int z0 = zt * TZ;
         const int z = z0 + lane;
         const int cur = k & 1;
         // prefetch the next tile's input moments into a register
         double mnext = 0.0;
         const int tn = t + gridDim.x;
-        if (coll && tid < NMOM * TZ && tn < nzt)
-            mnext = a.Min[(long long)(tid / TZ) * a.nz + tn * TZ + tid % TZ];
+        if (tid < NMOM * TZ && tn < nzt) {
+            int in2, zn;
+            tma_tile<BATCHED>(bd, tn, in2, zn);
+            const StageArgs &an = BATCHED ? bd.args[in2 * 4 + STAGE - 1] : a0;
+            if (an.flags & F_COLL)
+                mnext = an.Min[(long long)(tid / TZ) * an.nz + zn * TZ + tid % TZ];
+        }
         double macc[NMOM] = {0, 0, 0, 0, 0, 0};
         const double M0A = s_mom[cur][0][lane], M0B = s_mom[cur][1][lane],
                      M0C = s_mom[cur][2][lane], M1A = s_mom[cur][3][lane],
@@ -415,7 +461,7 @@ __global__ void __launch_bounds__(tma::NTHR, 1)
         }
         // tile epilogue: output moments (fixed-order sum over warps) and the
         // next tile's input moments
-        if (coll) {
+        if (coll || BATCHED) {
 #pragma unroll
             for (int m = 0; m < NMOM; ++m) s_red[warp][m][lane] = macc[m];
             consumer_sync();
@@ -424,7 +470,7 @@ __global__ void __launch_bounds__(tma::NTHR, 1)
                 double s = 0.0;
 #pragma unroll
                 for (int w = 0; w < R; ++w) s += s_red[w][m][zz];
-                a.Mout[(long long)m * a.nz + z0 + zz] = s;
+                if (coll) a.Mout[(long long)m * a.nz + z0 + zz] = s;
                 s_mom[cur ^ 1][m][zz] = mnext;
             }
             consumer_sync();
@@ -475,43 +521,54 @@ int make_state_map(CUtensorMap *map, const void *base, int elem_bytes, int ld, i
 int tma_box_x() { return tma::XW; }
 int tma_box_tile() { return tma::TZ; }
 // largest nvz the per-row tables in shared memory allow
-int tma_max_nvz() { return 1024; }
+int tma_max_nvz() { return TMA_MAX_NVZ; }
 
 static const int TMA_SMEM_MAX = 232448;  // opt-in shared memory per block on sm_100
 
 template <int SCHEME, bool GEN, int STAGE, class TC, class TIN, class TOUT>
 static cudaError_t launch_one(const CUtensorMap &mX, const CUtensorMap &mY, const CUtensorMap &mA,
-                              const StageArgs &a, int *err, int nblocks, cudaStream_t s)
+                              const StageArgs &a, int *err, int nblocks, cudaStream_t s,
+                              const BatchDev *bd, int max_nvz)
 {
     using L = tma::Layout<TIN, STAGE>;
-    constexpr int FIXED = (2 + tma::R) * NMOM * tma::TZ * 8 + 2 * 1024 * 8 + 1024;
+    constexpr int FIXED = (2 + tma::R) * NMOM * tma::TZ * 8 + 2 * TMA_MAX_NVZ * 8 + 1024;
     constexpr int NB = (L::BUF * 4 + FIXED <= TMA_SMEM_MAX) ? 4 : 3;
-    auto kern = rk4_stage_tma_kernel<SCHEME, GEN, STAGE, TC, TIN, TOUT, NB>;
-    if (nblocks <= 0)  // preparation call: raise the dynamic shared-memory limit
-        return cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, TMA_SMEM_MAX);
-    const int shmem = NB * L::BUF + 2 * NB * 8 + (2 + tma::R) * NMOM * tma::TZ * 8 + 2 * a.nvz * 8;
-    kern<<<nblocks, tma::NTHR, shmem, s>>>(mX, mY, mA, a, err);
+    auto kern = rk4_stage_tma_kernel<SCHEME, GEN, STAGE, TC, TIN, TOUT, NB, false>;
+    auto kernb = rk4_stage_tma_kernel<SCHEME, GEN, STAGE, TC, TIN, TOUT, NB, true>;
+    if (nblocks <= 0) {  // preparation call: raise the dynamic shared-memory limit
+        cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             TMA_SMEM_MAX);
+        if (e != cudaSuccess) return e;
+        return cudaFuncSetAttribute(kernb, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    TMA_SMEM_MAX);
+    }
+    const int shmem = NB * L::BUF + 2 * NB * 8 + (2 + tma::R) * NMOM * tma::TZ * 8 +
+                      (TMA_MAX_NVZ + max_nvz) * 8;
+    if (bd)
+        kernb<<<nblocks, tma::NTHR, shmem, s>>>(mX, mY, mA, a, err, *bd);
+    else
+        kern<<<nblocks, tma::NTHR, shmem, s>>>(mX, mY, mA, a, err, BatchDev{});
     return cudaGetLastError();
 }
 
 template <int SCHEME, bool GEN>
 static cudaError_t launch_p(const CUtensorMap &mX, const CUtensorMap &mY, const CUtensorMap &mA,
                             const StageArgs &a, int stage, int fp32, int *err, int nblocks,
-                            cudaStream_t s)
+                            cudaStream_t s, const BatchDev *bd, int max_nvz)
 {
     if (fp32) {
         switch (stage) {
-        case 1: return launch_one<SCHEME, GEN, 1, float, double, float>(mX, mY, mA, a, err, nblocks, s);
-        case 2: return launch_one<SCHEME, GEN, 2, float, float, float>(mX, mY, mA, a, err, nblocks, s);
-        case 3: return launch_one<SCHEME, GEN, 3, float, float, float>(mX, mY, mA, a, err, nblocks, s);
-        case 4: return launch_one<SCHEME, GEN, 4, float, float, double>(mX, mY, mA, a, err, nblocks, s);
+        case 1: return launch_one<SCHEME, GEN, 1, float, double, float>(mX, mY, mA, a, err, nblocks, s, bd, max_nvz);
+        case 2: return launch_one<SCHEME, GEN, 2, float, float, float>(mX, mY, mA, a, err, nblocks, s, bd, max_nvz);
+        case 3: return launch_one<SCHEME, GEN, 3, float, float, float>(mX, mY, mA, a, err, nblocks, s, bd, max_nvz);
+        case 4: return launch_one<SCHEME, GEN, 4, float, float, double>(mX, mY, mA, a, err, nblocks, s, bd, max_nvz);
         }
     } else {
         switch (stage) {
-        case 1: return launch_one<SCHEME, GEN, 1, double, double, double>(mX, mY, mA, a, err, nblocks, s);
-        case 2: return launch_one<SCHEME, GEN, 2, double, double, double>(mX, mY, mA, a, err, nblocks, s);
-        case 3: return launch_one<SCHEME, GEN, 3, double, double, double>(mX, mY, mA, a, err, nblocks, s);
-        case 4: return launch_one<SCHEME, GEN, 4, double, double, double>(mX, mY, mA, a, err, nblocks, s);
+        case 1: return launch_one<SCHEME, GEN, 1, double, double, double>(mX, mY, mA, a, err, nblocks, s, bd, max_nvz);
+        case 2: return launch_one<SCHEME, GEN, 2, double, double, double>(mX, mY, mA, a, err, nblocks, s, bd, max_nvz);
+        case 3: return launch_one<SCHEME, GEN, 3, double, double, double>(mX, mY, mA, a, err, nblocks, s, bd, max_nvz);
+        case 4: return launch_one<SCHEME, GEN, 4, double, double, double>(mX, mY, mA, a, err, nblocks, s, bd, max_nvz);
         }
     }
     return cudaErrorInvalidValue;
@@ -521,10 +578,25 @@ cudaError_t launch_rk4_stage_tma(const CUtensorMap &mX, const CUtensorMap &mY,
                                  const CUtensorMap &mA, const StageArgs &a, int scheme, int stage,
                                  int fp32, int *err, int nblocks, cudaStream_t s)
 {
-    if (scheme == FV) return launch_p<FV, false>(mX, mY, mA, a, stage, fp32, err, nblocks, s);
+    if (scheme == FV)
+        return launch_p<FV, false>(mX, mY, mA, a, stage, fp32, err, nblocks, s, nullptr, a.nvz);
     const bool gen = a.fd_advec != 0 || a.ko_order == 5;
-    return gen ? launch_p<FD, true>(mX, mY, mA, a, stage, fp32, err, nblocks, s)
-               : launch_p<FD, false>(mX, mY, mA, a, stage, fp32, err, nblocks, s);
+    return gen ? launch_p<FD, true>(mX, mY, mA, a, stage, fp32, err, nblocks, s, nullptr, a.nvz)
+               : launch_p<FD, false>(mX, mY, mA, a, stage, fp32, err, nblocks, s, nullptr, a.nvz);
+}
+
+// Ensemble launch: `a` carries the variant switches shared by every instance
+// (scheme variant, precision); per-instance values come from bd.
+cudaError_t launch_rk4_stage_tma_batch(const BatchDev &bd, const StageArgs &a, int scheme,
+                                       int stage, int fp32, int *err, int nblocks, int max_nvz,
+                                       cudaStream_t s)
+{
+    CUtensorMap m{};
+    if (scheme == FV)
+        return launch_p<FV, false>(m, m, m, a, stage, fp32, err, nblocks, s, &bd, max_nvz);
+    const bool gen = a.fd_advec != 0 || a.ko_order == 5;
+    return gen ? launch_p<FD, true>(m, m, m, a, stage, fp32, err, nblocks, s, &bd, max_nvz)
+               : launch_p<FD, false>(m, m, m, a, stage, fp32, err, nblocks, s, &bd, max_nvz);
 }
 
 // Sets the shared-memory attribute of every instantiation on the current device.
@@ -538,7 +610,8 @@ cudaError_t tma_prepare()
                 for (int st = 1; st <= 4; ++st) {
                     a.fd_advec = gen;
                     a.ko_order = 3;
-                    cudaError_t e = launch_rk4_stage_tma(m, m, m, a, sch, st, fp32, nullptr, 0, nullptr);
+                    cudaError_t e = launch_rk4_stage_tma(m, m, m, a, sch, st, fp32, nullptr, 0,
+                                                         nullptr);
                     if (e != cudaSuccess) return e;
                 }
     return cudaSuccess;

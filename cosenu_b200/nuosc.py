@@ -59,6 +59,21 @@ class NuOsc:
         if rc != L.OK:
             raise L.CosenuError(rc, self.lib.cosenu_last_error(None).decode())
         self.h = h
+        self._owned = True
+        self._init_grid()
+
+    @classmethod
+    def _member(cls, handle: int, params: L.Params) -> "NuOsc":
+        """View of an ensemble member (the ensemble owns the context)."""
+        self = cls.__new__(cls)
+        self.lib = L.load()
+        self.p = params
+        self.h = C.c_void_p(handle)
+        self._owned = False
+        self._init_grid()
+        return self
+
+    def _init_grid(self):
         g = (C.c_double * 5)()
         self.lib.cosenu_grid(self.h, g)
         self.dz, self.dv, self.dt, self.ct, self.st = list(g)
@@ -71,7 +86,8 @@ class NuOsc:
 
     def close(self) -> None:
         if getattr(self, "h", None):
-            self.lib.cosenu_destroy(self.h)
+            if getattr(self, "_owned", True):
+                self.lib.cosenu_destroy(self.h)
             self.h = None
 
     def __del__(self):

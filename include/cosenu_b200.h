@@ -192,6 +192,38 @@ int cosenu_device_state(cosenu_ctx *ctx, double *comp[8], int *ld);
 int cosenu_upload_device(cosenu_ctx *ctx, const double *const comp[8], int ld);
 int cosenu_download_device(cosenu_ctx *ctx, double *const comp[8], int ld);
 
+/* ---------------------------------------------------------------------------
+ * Ensembles (no counterpart in the reference, which runs one configuration per
+ * process: manage.py:361-428 submits one job per (nz, nvz, CFL)).  Many
+ * independent simulations of uneven nz, nvz and physics advance together:
+ * one launch per RK4 stage covers every member with steps left.  Members are
+ * ordinary contexts (cosenu_batch_member) for initial conditions, analysis and
+ * download.  Members must share scheme, FD variant, precision and device, and
+ * need nz % 32 == 0, nvz <= 1024. */
+typedef struct cosenu_batch cosenu_batch;
+int cosenu_batch_create(int n, const cosenu_params *params, cosenu_batch **out);
+int cosenu_batch_destroy(cosenu_batch *b);
+const char *cosenu_batch_last_error(const cosenu_batch *b);
+int cosenu_batch_size(const cosenu_batch *b);
+/* Runs the ensemble (and its members) on the given cudaStream_t. */
+int cosenu_batch_set_stream(cosenu_batch *b, void *cuda_stream);
+cosenu_ctx *cosenu_batch_member(cosenu_batch *b, int i);
+/* cosenu_init_seeded for every member (instance number = member index). */
+int cosenu_batch_init_seeded(cosenu_batch *b, const uint64_t *seeds, const double *sig_nu,
+                             const double *sig_nubar, const double *alpha, double amp);
+/* Advances member i by nsteps[i] RK4 steps (asynchronous). */
+int cosenu_batch_run(cosenu_batch *b, const long long *nsteps);
+int cosenu_batch_synchronize(cosenu_batch *b);
+/* Times trial_steps ensemble steps for each candidate kernel family and tile
+ * (TMA-pipelined; register-tiled with z tile 32/16/8 and a v tile per nvz
+ * class) and keeps the fastest; member states are restored.  A text report of
+ * the timings goes to `report` (may be NULL). */
+int cosenu_batch_autotune(cosenu_batch *b, int trial_steps, char *report, size_t report_len);
+/* Current / explicit kernel choice (use_tma 1: TMA-pipelined; 0: register-
+ * tiled with z tile tz and v tile tv_per_member[i]). */
+int cosenu_batch_config(const cosenu_batch *b, int *use_tma, int *tz, int *tv_per_member);
+int cosenu_batch_set_config(cosenu_batch *b, int use_tma, int tz, const int *tv_per_member);
+
 /* For callers that must not allocate device memory (a host application whose
  * device memory all comes from its own pool, or a loop that cannot afford the
  * device synchronisation cudaMalloc/cudaFree may cause).  No counterpart in the

@@ -454,6 +454,66 @@ def run_ensemble(args):
     }), flush=True)
 
 
+def run_fp32_study(args):
+    """the FP32-bulk form against the FP64 form on the same seeded
+    input: max-abs error per component at the end, <Pee>(t) error, trace and
+    ELN drift of both, and the throughput of each (timed separately)."""
+    import numpy as np
+    import torch
+
+    from cosenu_b200 import NuOsc
+
+    torch.cuda.set_device(0)
+    stream = torch.cuda.Stream()
+    torch.cuda.set_stream(stream)
+    n, every = args.study_steps, max(1, args.study_steps // 20)
+    out = {}
+    sims = {}
+    for prec in ("fp64", "fp32"):
+        sim = NuOsc(precision=prec, **WORKLOAD)
+        sim.set_stream(stream.cuda_stream)
+        sim.init_seeded(SEED, **IC)
+        sims[prec] = sim
+    hist = {"fp64": [], "fp32": []}
+    times = {"fp64": 0.0, "fp32": 0.0}
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a0 = {p: sims[p].analyse() for p in sims}
+    done = 0
+    while done < n:
+        k = min(every, n - done)
+        for prec, sim in sims.items():
+            e0.record(stream)
+            sim.evolve(k)
+            e1.record(stream)
+            torch.cuda.synchronize()
+            times[prec] += e0.elapsed_time(e1) / 1e3
+            hist[prec].append(sim.analyse())
+        done += k
+    st = {p: sims[p].download() for p in sims}
+    gz = WORKLOAD["gz"]
+    err = np.abs(st["fp32"][:, :, gz:-gz] - st["fp64"][:, :, gz:-gz]).reshape(8, -1).max(axis=1)
+    dpee = max(abs(a["Pee"] - b["Pee"]) for a, b in zip(hist["fp32"], hist["fp64"]))
+    dpbee = max(abs(a["Pbee"] - b["Pbee"]) for a, b in zip(hist["fp32"], hist["fp64"]))
+    drift = {p: {"trace": abs(hist[p][-1]["trace"] - a0[p]["trace"]) / abs(a0[p]["trace"]),
+                 "btrace": abs(hist[p][-1]["btrace"] - a0[p]["btrace"]) / abs(a0[p]["btrace"]),
+                 "eln": abs(hist[p][-1]["eln"] - a0[p]["eln"]) / abs(a0[p]["eln"])}
+             for p in sims}
+    cells = WORKLOAD["nz"] * WORKLOAD["nvz"]
+    print(json.dumps({
+        "study": "FP32-bulk vs FP64", "workload": WORKLOAD_NAMES[args.workload],
+        "steps": n, "t_end": n * sims["fp64"].dt,
+        "max_abs_err_per_component": dict(zip(("ee", "xx", "ex_re", "ex_im", "bee", "bxx",
+                                                "bex_re", "bex_im"), err.tolist())),
+        "max_abs_err_Pee_t": dpee, "max_abs_err_Pbee_t": dpbee,
+        "final_Pee": {p: hist[p][-1]["Pee"] for p in sims},
+        "relative_drift": drift,
+        "cell_updates_per_s": {p: cells * n / times[p] for p in sims},
+        "speedup_fp32_over_fp64": times["fp64"] / times["fp32"],
+    }), flush=True)
+    for s_ in sims.values():
+        s_.close()
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -462,6 +522,9 @@ def main():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--instances", type=int, default=256, help="c4: ensemble size")
+    ap.add_argument("--fp32-study", action="store_true",
+                    help="FP32-bulk vs FP64 error study on the chosen workload")
+    ap.add_argument("--study-steps", type=int, default=8000)
     ap.add_argument("--t-factor", type=float, default=1000.0, help="c4: run to t_factor/mu")
     ap.add_argument("--workload", choices=sorted(WORKLOADS) + ["c4"], default="c2",
                     help="c2 (default, the headline): FD 32768 x 256; c1: FV 1024 x 64; "
@@ -481,6 +544,9 @@ def main():
     if args.nz != WORKLOAD["nz"]:
         dz = (WORKLOAD["z1"] - WORKLOAD["z0"]) / WORKLOAD["nz"]
         WORKLOAD.update(nz=args.nz, z0=-0.5 * args.nz * dz, z1=0.5 * args.nz * dz)
+    if args.fp32_study:
+        run_fp32_study(args)
+        return
     if args.warmup < 3 and args.impl == "ours":
         args.warmup = 3
     if args.impl == "reference":

@@ -38,7 +38,7 @@ struct cosenu_batch {
     StageArgs *d_args = nullptr;
     CUtensorMap *d_maps = nullptr;
     int4 *d_table[2] = {nullptr, nullptr};
-    int4 *h_table[2] = {nullptr, nullptr};  // pinned staging
+    int4 *h_table[2] = {nullptr, nullptr};  // pinned staging (table, then block ranges)
     cudaEvent_t table_ev[2] = {nullptr, nullptr};
     size_t table_cap = 0;
     int phase = 0;
@@ -79,10 +79,37 @@ int upload_args(cosenu_batch *b)
     return COSENU_OK;
 }
 
-// Table of tiles of the members in `active`, heaviest tiles first.
-size_t build_table(cosenu_batch *b, const std::vector<int> &active, std::vector<int4> &out)
+// Table of tiles of the members in `active`.  TMA family: member by member
+// (a block then streams consecutive z tiles of one member), with `ranges`
+// splitting the table into nblk contiguous pieces of equal work; register-
+// tiled family: heaviest tiles first (one block per entry).
+size_t build_table(cosenu_batch *b, const std::vector<int> &active, std::vector<int4> &out,
+                   std::vector<int> *ranges = nullptr, int nblk = 0)
 {
     out.clear();
+    if (b->use_tma) {
+        std::vector<long long> w;
+        for (int i : active) {
+            const cosenu_params &p = b->m[i]->p;
+            for (int zt = 0; zt < p.nz / 32; ++zt) {
+                out.push_back(make_int4(i, zt, 0, 0));
+                w.push_back((long long)(p.nvz + 7) / 8 + 1);  // chunks + per-tile overhead
+            }
+        }
+        if (ranges) {
+            long long total = 0;
+            for (long long x : w) total += x;
+            ranges->assign(nblk + 1, (int)out.size());
+            (*ranges)[0] = 0;
+            long long acc = 0;
+            int blk = 1;
+            for (size_t t = 0; t < out.size() && blk < nblk; ++t) {
+                acc += w[t];
+                while (blk < nblk && acc * nblk >= total * blk) (*ranges)[blk++] = (int)t + 1;
+            }
+        }
+        return out.size();
+    }
     std::vector<std::pair<long long, int4>> t;
     for (int i : active) {
         const cosenu_params &p = b->m[i]->p;
@@ -123,17 +150,25 @@ int ensure_table_cap(cosenu_batch *b, size_t n)
 int run_phase(cosenu_batch *b, const std::vector<int> &active, long long nsteps)
 {
     std::vector<int4> tab;
-    size_t nt = build_table(b, active, tab);
+    std::vector<int> ranges;
+    size_t ntiles_all = 0;
+    for (int i : active) ntiles_all += b->m[i]->p.nz / 32;
+    const int nblk = (int)std::min<size_t>(std::max<size_t>(ntiles_all, 1), (size_t)b->nsm);
+    size_t nt = build_table(b, active, tab, &ranges, nblk);
     if (nt == 0 || nsteps <= 0) return COSENU_OK;
-    int rc = ensure_table_cap(b, nt);
+    // table entries, then (TMA family) the nblk + 1 block range starts
+    const size_t nrange_int4 = b->use_tma ? (ranges.size() + 3) / 4 : 0;
+    int rc = ensure_table_cap(b, nt + nrange_int4);
     if (rc) return rc;
     const int k = b->phase++ & 1;
     BCK(cudaEventSynchronize(b->table_ev[k]));  // staging buffer free again
     std::memcpy(b->h_table[k], tab.data(), nt * sizeof(int4));
-    BCK(cudaMemcpyAsync(b->d_table[k], b->h_table[k], nt * sizeof(int4), cudaMemcpyHostToDevice,
-                        b->stream));
+    if (nrange_int4) std::memcpy(b->h_table[k] + nt, ranges.data(), ranges.size() * sizeof(int));
+    BCK(cudaMemcpyAsync(b->d_table[k], b->h_table[k], (nt + nrange_int4) * sizeof(int4),
+                        cudaMemcpyHostToDevice, b->stream));
     BCK(cudaEventRecord(b->table_ev[k], b->stream));
-    BatchDev bd{b->d_table[k], (int)nt, b->d_args, b->d_maps};
+    BatchDev bd{b->d_table[k], (int)nt, b->d_args, b->d_maps,
+                reinterpret_cast<const int *>(b->d_table[k] + nt)};
     int max_nvz = 0;
     for (int i : active) max_nvz = std::max(max_nvz, b->m[i]->p.nvz);
     const StageArgs a0 = ctx_stage_args(b->m[active[0]], 1);
@@ -141,8 +176,8 @@ int run_phase(cosenu_batch *b, const std::vector<int> &active, long long nsteps)
         for (int st = 1; st <= 4; ++st) {
             cudaError_t e;
             if (b->use_tma)
-                e = launch_rk4_stage_tma_batch(bd, a0, b->scheme, st, b->fp32, b->err_flag,
-                                               (int)std::min<size_t>(nt, (size_t)b->nsm), max_nvz, s);
+                e = launch_rk4_stage_tma_batch(bd, a0, b->scheme, st, b->fp32, b->err_flag, nblk,
+                                               max_nvz, s);
             else
                 e = launch_rk4_stage_batch(bd, b->scheme, st, b->tz, b->fp32, s);
             if (e != cudaSuccess) return e;

@@ -53,6 +53,7 @@ struct BatchDev {
     int ntiles;
     const StageArgs *args;      // [instances][4]
     const CUtensorMap *maps;    // [instances][5]
+    const int *range;           // TMA family: block b owns table entries [range[b], range[b+1])
 };
 
 // Layout helpers shared by host and device code.

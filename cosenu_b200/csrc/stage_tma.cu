@@ -172,7 +172,10 @@ __global__ void __launch_bounds__(tma::NTHR, 1)
         // ------------------------------------------------------------ producer
         if (lane == 0) {
             uint32_t it = 0;
-            for (int t = blockIdx.x; t < nzt; t += gridDim.x) {
+            const int t_first = BATCHED ? bd.range[blockIdx.x] : blockIdx.x;
+            const int t_end = BATCHED ? bd.range[blockIdx.x + 1] : nzt;
+            const int t_step = BATCHED ? 1 : gridDim.x;
+            for (int t = t_first; t < t_end; t += t_step) {
                 int inst, zt;
                 tma_tile<BATCHED>(bd, t, inst, zt);
                 const StageArgs &a = BATCHED ? bd.args[inst * 4 + STAGE - 1] : a0;
@@ -204,11 +207,16 @@ __global__ void __launch_bounds__(tma::NTHR, 1)
             s_vz[i] = a0.vz[i];
             s_fac[i] = a0.rowfac[i];
         }
+    // this block's tiles: a contiguous range of the ensemble table, or every
+    // gridDim.x-th z tile of a single simulation
+    const int t_first = BATCHED ? bd.range[blockIdx.x] : blockIdx.x;
+    const int t_end = BATCHED ? bd.range[blockIdx.x + 1] : nzt;
+    const int t_step = BATCHED ? 1 : gridDim.x;
     // moments of the stage input for the first tile
     int k = 0;
-    if ((int)blockIdx.x < nzt && tid < NMOM * TZ) {
+    if (t_first < t_end && tid < NMOM * TZ) {
         int inst, zt;
-        tma_tile<BATCHED>(bd, blockIdx.x, inst, zt);
+        tma_tile<BATCHED>(bd, t_first, inst, zt);
         const StageArgs &a = BATCHED ? bd.args[inst * 4 + STAGE - 1] : a0;
         if (a.flags & F_COLL)
             s_mom[0][tid / TZ][tid % TZ] = a.Min[(long long)(tid / TZ) * a.nz + zt * TZ + tid % TZ];
@@ -217,7 +225,7 @@ __global__ void __launch_bounds__(tma::NTHR, 1)
 
     uint32_t it = 0;
     int prev_inst = -1;
-    for (int t = blockIdx.x; t < nzt; t += gridDim.x, ++k) {
+    for (int t = t_first; t < t_end; t += t_step, ++k) {
         int inst, zt;
         tma_tile<BATCHED>(bd, t, inst, zt);
         const StageArgs &a = BATCHED ? bd.args[inst * 4 + STAGE - 1] : a0;
@@ -243,8 +251,8 @@ __global__ void __launch_bounds__(tma::NTHR, 1)
         const int cur = k & 1;
         // prefetch the next tile's input moments into a register
         double mnext = 0.0;
-        const int tn = t + gridDim.x;
-        if (tid < NMOM * TZ && tn < nzt) {
+        const int tn = t + t_step;
+        if (tid < NMOM * TZ && tn < t_end) {
             int in2, zn;
             tma_tile<BATCHED>(bd, tn, in2, zn);
             const StageArgs &an = BATCHED ? bd.args[in2 * 4 + STAGE - 1] : a0;

@@ -514,6 +514,60 @@ def run_fp32_study(args):
         s_.close()
 
 
+def run_surrogate(args):
+    """configs[4] (reduced): solver targets for a training and a
+    held-out set, a committee of networks trained on the GPU, held-out error
+    against the solver with and without the disagreement fallback, and the
+    time of both routes."""
+    import numpy as np
+    import torch
+
+    from cosenu_b200.surrogate import Surrogate, features, solve_pee, surrogate_instances
+
+    torch.cuda.set_device(0)
+    train = surrogate_instances(args.train, seed=21, nz=args.sur_nz, t_factor=args.t_factor)
+    test = surrogate_instances(args.test, seed=22, nz=args.sur_nz, t_factor=args.t_factor)
+    t0 = time.perf_counter()
+    y_train = solve_pee(train)
+    t_train_data = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    y_test = solve_pee(test)
+    torch.cuda.synchronize()
+    t_solver = time.perf_counter() - t0
+    x_train = np.stack([features(i) for i in train])
+    x_test = np.stack([features(i) for i in test])
+    sur = Surrogate(n_models=4)
+    t0 = time.perf_counter()
+    losses = sur.fit(x_train, y_train, epochs=args.epochs, batch=256, lr=1e-3)
+    t_fit = time.perf_counter() - t0
+    sur.committee(x_test[:8])  # warm-up
+    t0 = time.perf_counter()
+    mean, spread = sur.committee(x_test)
+    t_net = time.perf_counter() - t0
+    err = np.abs(mean - y_test)
+    fb = spread > args.threshold
+    final = mean.copy()
+    final[fb] = y_test[fb]  # the solver's own answer where the committee falls back
+    t_with_fb = t_net + t_solver * fb.mean()
+    err_fb = np.abs(final - y_test)
+    print(json.dumps({
+        "metric": "surrogate vs solver on held-out instances", "train": len(train),
+        "test": len(test), "nz": args.sur_nz, "nvz": 128, "t_factor": args.t_factor,
+        "mean_abs_err": float(err.mean()), "rms_err": float(np.sqrt((err ** 2).mean())),
+        "p95_instance_max_err": float(np.percentile(err.max(axis=1), 95)),
+        "fallback_threshold": args.threshold, "fallback_fraction": float(fb.mean()),
+        "mean_abs_err_with_fallback": float(err_fb.mean()),
+        "baseline_mean_abs_err_train_average": float(np.abs(y_train.mean(0) - y_test).mean()),
+        "baseline_mean_abs_err_no_conversion": float(np.abs(1.0 - y_test).mean()),
+        "solver_seconds_test": t_solver, "surrogate_seconds_test": t_net,
+        "speedup_surrogate_only": t_solver / t_net,
+        "speedup_with_fallback": t_solver / t_with_fb,
+        "train_data_seconds": t_train_data, "train_seconds": t_fit,
+        "final_train_loss": [float(ls[-1]) for ls in losses],
+    }), flush=True)
+    sur.close()
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -522,11 +576,16 @@ def main():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--instances", type=int, default=256, help="c4: ensemble size")
+    ap.add_argument("--train", type=int, default=2048, help="c5: training instances")
+    ap.add_argument("--test", type=int, default=512, help="c5: held-out instances")
+    ap.add_argument("--sur-nz", type=int, default=512, help="c5: nz of the solver runs")
+    ap.add_argument("--epochs", type=int, default=300, help="c5: training epochs")
+    ap.add_argument("--threshold", type=float, default=1e-2, help="c5: fallback threshold")
     ap.add_argument("--fp32-study", action="store_true",
                     help="FP32-bulk vs FP64 error study on the chosen workload")
     ap.add_argument("--study-steps", type=int, default=8000)
     ap.add_argument("--t-factor", type=float, default=1000.0, help="c4: run to t_factor/mu")
-    ap.add_argument("--workload", choices=sorted(WORKLOADS) + ["c4"], default="c2",
+    ap.add_argument("--workload", choices=sorted(WORKLOADS) + ["c4", "c5"], default="c2",
                     help="c2 (default, the headline): FD 32768 x 256; c1: FV 1024 x 64; "
                          "c3: FV 65536 x 512")
     ap.add_argument("--precision", choices=["fp64", "fp32"], default="fp64")
@@ -536,6 +595,9 @@ def main():
     args = ap.parse_args()
     if args.workload == "c4":
         run_ensemble(args)
+        return
+    if args.workload == "c5":
+        run_surrogate(args)
         return
     WORKLOAD.clear()
     WORKLOAD.update(WORKLOADS[args.workload])

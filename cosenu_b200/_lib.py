@@ -32,6 +32,9 @@ EXPORTS = (
     "cosenu_batch_size", "cosenu_batch_member", "cosenu_batch_init_seeded", "cosenu_batch_run",
     "cosenu_batch_synchronize", "cosenu_batch_autotune", "cosenu_batch_config",
     "cosenu_batch_set_config", "cosenu_batch_set_stream",
+    "cosenu_mlp_create", "cosenu_mlp_destroy", "cosenu_mlp_last_error", "cosenu_mlp_num_params",
+    "cosenu_mlp_get_params", "cosenu_mlp_set_params", "cosenu_mlp_forward",
+    "cosenu_mlp_loss_grad", "cosenu_mlp_set_data", "cosenu_mlp_train",
 )
 
 
@@ -116,6 +119,17 @@ def load(path: str | None = None) -> C.CDLL:
         "cosenu_batch_config": (i, [vp, C.POINTER(i), C.POINTER(i), vp]),
         "cosenu_batch_set_config": (i, [vp, i, i, vp]),
         "cosenu_batch_set_stream": (i, [vp, vp]),
+        "cosenu_mlp_create": (i, [i, i, i, i, C.c_uint64, i, C.POINTER(vp)]),
+        "cosenu_mlp_destroy": (i, [vp]),
+        "cosenu_mlp_last_error": (C.c_char_p, [vp]),
+        "cosenu_mlp_num_params": (i, [vp, C.POINTER(C.c_size_t)]),
+        "cosenu_mlp_get_params": (i, [vp, vp]),
+        "cosenu_mlp_set_params": (i, [vp, vp]),
+        "cosenu_mlp_forward": (i, [vp, vp, i, vp]),
+        "cosenu_mlp_loss_grad": (i, [vp, vp, vp, i, C.POINTER(C.c_float), vp]),
+        "cosenu_mlp_set_data": (i, [vp, vp, vp, i]),
+        "cosenu_mlp_train": (i, [vp, i, i, C.c_float, C.c_float, C.c_float, C.c_float,
+                                 C.c_float, C.c_uint64, vp]),
     }
     for name, (res, args) in sig.items():
         f = getattr(lib, name)

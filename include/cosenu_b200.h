@@ -224,6 +224,31 @@ int cosenu_batch_autotune(cosenu_batch *b, int trial_steps, char *report, size_t
 int cosenu_batch_config(const cosenu_batch *b, int *use_tma, int *tz, int *tv_per_member);
 int cosenu_batch_set_config(cosenu_batch *b, int use_tma, int tz, const int *tv_per_member);
 
+/* ---------------------------------------------------------------------------
+ * Surrogate network (no counterpart in the reference): fully connected,
+ * n_in -> n_hidden x n_hidden_layers -> n_out with GELU between layers, BF16
+ * weights and activations on the tensor cores with FP32 accumulation, FP32
+ * master weights trained by AdamW on the mean-squared error.  Parameters are
+ * one flat FP32 vector: for each layer W [out][in] (in padded to a multiple
+ * of 16, padding columns zero) then b [out]. */
+typedef struct cosenu_mlp cosenu_mlp;
+int cosenu_mlp_create(int n_in, int n_hidden, int n_hidden_layers, int n_out, uint64_t seed,
+                      int device, cosenu_mlp **out);
+int cosenu_mlp_destroy(cosenu_mlp *net);
+const char *cosenu_mlp_last_error(const cosenu_mlp *net);
+int cosenu_mlp_num_params(const cosenu_mlp *net, size_t *n);
+int cosenu_mlp_get_params(cosenu_mlp *net, float *host);
+int cosenu_mlp_set_params(cosenu_mlp *net, const float *host);
+/* y [rows][n_out] for x [rows][n_in] (host arrays). */
+int cosenu_mlp_forward(cosenu_mlp *net, const float *x_host, int rows, float *y_host);
+/* Loss 1/(rows*n_out) sum (y - t)^2 and its gradient (flat, like the params). */
+int cosenu_mlp_loss_grad(cosenu_mlp *net, const float *x_host, const float *t_host, int rows,
+                         float *loss, float *grad_host);
+/* Training data held on the device, then minibatch AdamW epochs over it. */
+int cosenu_mlp_set_data(cosenu_mlp *net, const float *x_host, const float *t_host, int n);
+int cosenu_mlp_train(cosenu_mlp *net, int epochs, int batch, float lr, float weight_decay,
+                     float beta1, float beta2, float eps, uint64_t shuffle_seed, float *epoch_loss);
+
 /* For callers that must not allocate device memory (a host application whose
  * device memory all comes from its own pool, or a loop that cannot afford the
  * device synchronisation cudaMalloc/cudaFree may cause).  No counterpart in the

@@ -418,6 +418,7 @@ def run_ensemble(args):
     # plain path: every 8th instance alone, FP64, default kernel choice
     sub = list(range(0, len(xs), 8))
     t_sub = 0.0
+    pee_err = 0.0
     for i in sub:
         x = xs[i]
         sim = NuOsc(nz=x.nz, nvz=x.nvz, gz=4, z0=x.z0, z1=x.z1, cfl=x.cfl, omega=0.0, mu=x.mu,
@@ -435,6 +436,8 @@ def run_ensemble(args):
             d = abs(sim.analyse()["Pee"] - pee[i])
             if d > 1e-9:
                 raise SystemExit(f"ensemble member {i} differs from the plain path: {d}")
+        else:
+            pee_err = max(pee_err, abs(sim.analyse()["Pee"] - pee[i]))
         sim.close()
     w_sub = sum(work[i] for i in sub)
     t_plain = t_sub * sum(work) / w_sub
@@ -446,6 +449,7 @@ def run_ensemble(args):
         "plain_fp64_instances_per_s": n / t_plain,
         "plain_fp64_note": f"{len(sub)} of {n} instances run alone ({t_sub:.1f} s), scaled by work",
         "speedup_vs_plain": t_plain / t_batch, "higher_is_better": True,
+        "max_abs_err_final_Pee_vs_plain_fp64": pee_err if args.precision != "fp64" else 0.0,
         "precision": args.precision.upper(), "data": "synthetic",
         "config": {"workload": "256 FV WENO7 instances, nz logU[512,8192]/256, nvz {32..256}, "
                                "alpha U[.6,1.2], sigma U[.4,.8]/U[.3,.7], mu U[.5,2], "

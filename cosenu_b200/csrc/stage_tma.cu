@@ -152,9 +152,9 @@ __global__ void __launch_bounds__(tma::NTHR, 1)
     uint64_t *full = reinterpret_cast<uint64_t *>(smem + NBUF * L::BUF);
     uint64_t *empty = full + NBUF;
     double(*s_mom)[NMOM][TZ] = reinterpret_cast<double(*)[NMOM][TZ]>(empty + NBUF);
-    double(*s_red)[NMOM][TZ] = s_mom + 2;
-    double *s_vz = reinterpret_cast<double *>(s_red + R);  // [nvz] velocities
-    double *s_fac = s_vz + TMA_MAX_NVZ;                    // [nvz] advection factors
+    double(*s_red)[NMOM][TZ] = s_mom + 2;                   // [R/2][6][TZ]
+    double *s_vz = reinterpret_cast<double *>(s_red + R / 2);  // [tab] velocities
+    double *s_fac = s_vz + bd.tab;                             // [tab] advection factors
 
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const int nzt = BATCHED ? bd.ntiles : a0.nz / TZ;
@@ -470,14 +470,23 @@ __global__ void __launch_bounds__(tma::NTHR, 1)
         // tile epilogue: output moments (fixed-order sum over warps) and the
         // next tile's input moments
         if (coll || BATCHED) {
+            // warps w and w + R/2 pair up, then the R/2 pair sums are added
+            // in a fixed order
+            if (warp >= R / 2) {
 #pragma unroll
-            for (int m = 0; m < NMOM; ++m) s_red[warp][m][lane] = macc[m];
+                for (int m = 0; m < NMOM; ++m) s_red[warp - R / 2][m][lane] = macc[m];
+            }
+            consumer_sync();
+            if (warp < R / 2) {
+#pragma unroll
+                for (int m = 0; m < NMOM; ++m) s_red[warp][m][lane] += macc[m];
+            }
             consumer_sync();
             if (tid < NMOM * TZ) {
                 const int m = tid / TZ, zz = tid % TZ;
                 double s = 0.0;
 #pragma unroll
-                for (int w = 0; w < R; ++w) s += s_red[w][m][zz];
+                for (int w = 0; w < R / 2; ++w) s += s_red[w][m][zz];
                 if (coll) a.Mout[(long long)m * a.nz + z0 + zz] = s;
                 s_mom[cur ^ 1][m][zz] = mnext;
             }
@@ -533,14 +542,20 @@ int tma_max_nvz() { return TMA_MAX_NVZ; }
 
 static const int TMA_SMEM_MAX = 232448;  // opt-in shared memory per block on sm_100
 
-template <int SCHEME, bool GEN, int STAGE, class TC, class TIN, class TOUT>
-static cudaError_t launch_one(const CUtensorMap &mX, const CUtensorMap &mY, const CUtensorMap &mA,
-                              const StageArgs &a, int *err, int nblocks, cudaStream_t s,
-                              const BatchDev *bd, int max_nvz)
+// Shared memory of one block with an NB-deep ring and per-row tables for
+// `tab` rows.
+template <class TIN, int STAGE>
+static int tma_smem(int NB, int tab)
 {
     using L = tma::Layout<TIN, STAGE>;
-    constexpr int FIXED = (2 + tma::R) * NMOM * tma::TZ * 8 + 2 * TMA_MAX_NVZ * 8 + 1024;
-    constexpr int NB = (L::BUF * 4 + FIXED <= TMA_SMEM_MAX) ? 4 : 3;
+    return NB * L::BUF + 2 * NB * 8 + (2 + tma::R / 2) * NMOM * tma::TZ * 8 + 2 * tab * 8;
+}
+
+template <int SCHEME, bool GEN, int STAGE, class TC, class TIN, class TOUT, int NB>
+static cudaError_t launch_nb(const CUtensorMap &mX, const CUtensorMap &mY, const CUtensorMap &mA,
+                             const StageArgs &a, int *err, int nblocks, cudaStream_t s,
+                             const BatchDev *bd, int tab)
+{
     auto kern = rk4_stage_tma_kernel<SCHEME, GEN, STAGE, TC, TIN, TOUT, NB, false>;
     auto kernb = rk4_stage_tma_kernel<SCHEME, GEN, STAGE, TC, TIN, TOUT, NB, true>;
     if (nblocks <= 0) {  // preparation call: raise the dynamic shared-memory limit
@@ -550,13 +565,38 @@ static cudaError_t launch_one(const CUtensorMap &mX, const CUtensorMap &mY, cons
         return cudaFuncSetAttribute(kernb, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                     TMA_SMEM_MAX);
     }
-    const int shmem = NB * L::BUF + 2 * NB * 8 + (2 + tma::R) * NMOM * tma::TZ * 8 +
-                      (TMA_MAX_NVZ + max_nvz) * 8;
-    if (bd)
-        kernb<<<nblocks, tma::NTHR, shmem, s>>>(mX, mY, mA, a, err, *bd);
-    else
-        kern<<<nblocks, tma::NTHR, shmem, s>>>(mX, mY, mA, a, err, BatchDev{});
+    const int shmem = tma_smem<TIN, STAGE>(NB, tab);
+    if (bd) {
+        BatchDev b2 = *bd;
+        b2.tab = tab;
+        kernb<<<nblocks, tma::NTHR, shmem, s>>>(mX, mY, mA, a, err, b2);
+    } else {
+        BatchDev b2{};
+        b2.tab = tab;
+        kern<<<nblocks, tma::NTHR, shmem, s>>>(mX, mY, mA, a, err, b2);
+    }
     return cudaGetLastError();
+}
+
+// A 4-deep ring where it fits in shared memory (always, except FP64 stages 2
+// and 3 with more than ~600 rows), else 3-deep.
+template <int SCHEME, bool GEN, int STAGE, class TC, class TIN, class TOUT>
+static cudaError_t launch_one(const CUtensorMap &mX, const CUtensorMap &mY, const CUtensorMap &mA,
+                              const StageArgs &a, int *err, int nblocks, cudaStream_t s,
+                              const BatchDev *bd, int max_nvz)
+{
+    constexpr bool MAY_NEED_3 = (STAGE == 2 || STAGE == 3) && sizeof(TIN) == 8;
+    const int tab = (max_nvz + 7) / 8 * 8;
+    if (nblocks <= 0) {
+        cudaError_t e = launch_nb<SCHEME, GEN, STAGE, TC, TIN, TOUT, 4>(mX, mY, mA, a, err, 0, s, bd, tab);
+        if (e != cudaSuccess || !MAY_NEED_3) return e;
+        return launch_nb<SCHEME, GEN, STAGE, TC, TIN, TOUT, MAY_NEED_3 ? 3 : 4>(mX, mY, mA, a, err, 0,
+                                                                               s, bd, tab);
+    }
+    if (tma_smem<TIN, STAGE>(4, tab) <= TMA_SMEM_MAX || !MAY_NEED_3)
+        return launch_nb<SCHEME, GEN, STAGE, TC, TIN, TOUT, 4>(mX, mY, mA, a, err, nblocks, s, bd, tab);
+    return launch_nb<SCHEME, GEN, STAGE, TC, TIN, TOUT, MAY_NEED_3 ? 3 : 4>(mX, mY, mA, a, err,
+                                                                           nblocks, s, bd, tab);
 }
 
 template <int SCHEME, bool GEN>

@@ -526,7 +526,8 @@ def run_surrogate(args):
     import numpy as np
     import torch
 
-    from cosenu_b200.surrogate import Surrogate, features, solve_pee, surrogate_instances
+    from cosenu_b200.surrogate import (Surrogate, features, reseeded, solve_pee,
+                                       surrogate_instances)
 
     torch.cuda.set_device(0)
     train = surrogate_instances(args.train, seed=21, nz=args.sur_nz, t_factor=args.t_factor)
@@ -538,6 +539,9 @@ def run_surrogate(args):
     y_test = solve_pee(test)
     torch.cuda.synchronize()
     t_solver = time.perf_counter() - t0
+    # the solver's own seed-to-seed spread on the first 128 held-out set-ups
+    y_reseed = solve_pee(reseeded(test[:128]))
+    noise = float(np.abs(y_reseed - y_test[:128]).mean())
     x_train = np.stack([features(i) for i in train])
     x_test = np.stack([features(i) for i in test])
     sur = Surrogate(n_models=4)
@@ -561,6 +565,7 @@ def run_surrogate(args):
         "p95_instance_max_err": float(np.percentile(err.max(axis=1), 95)),
         "fallback_threshold": args.threshold, "fallback_fraction": float(fb.mean()),
         "mean_abs_err_with_fallback": float(err_fb.mean()),
+        "solver_seed_to_seed_mean_abs_diff": noise,
         "baseline_mean_abs_err_train_average": float(np.abs(y_train.mean(0) - y_test).mean()),
         "baseline_mean_abs_err_no_conversion": float(np.abs(1.0 - y_test).mean()),
         "solver_seconds_test": t_solver, "surrogate_seconds_test": t_net,
@@ -583,7 +588,7 @@ def main():
     ap.add_argument("--train", type=int, default=2048, help="c5: training instances")
     ap.add_argument("--test", type=int, default=512, help="c5: held-out instances")
     ap.add_argument("--sur-nz", type=int, default=512, help="c5: nz of the solver runs")
-    ap.add_argument("--epochs", type=int, default=300, help="c5: training epochs")
+    ap.add_argument("--epochs", type=int, default=900, help="c5: training epochs")
     ap.add_argument("--threshold", type=float, default=1e-2, help="c5: fallback threshold")
     ap.add_argument("--fp32-study", action="store_true",
                     help="FP32-bulk vs FP64 error study on the chosen workload")

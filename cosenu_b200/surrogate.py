@@ -37,6 +37,14 @@ def features(x: Instance) -> np.ndarray:
                            [x.alpha, x.mu]]).astype(np.float32)
 
 
+def reseeded(instances: list[Instance], offset: int = 7919) -> list[Instance]:
+    """The same physical set-ups with different random perturbations (the
+    seed-to-seed spread of the solver is the noise floor of any predictor of
+    P_ee(v) from the angular profiles alone)."""
+    import dataclasses
+    return [dataclasses.replace(x, seed=x.seed + offset) for x in instances]
+
+
 def surrogate_instances(n: int, seed: int, nz: int = 512, nvz: int = 128,
                         t_factor: float = 1000.0) -> list[Instance]:
     """configs[4] inputs: the configs[3] parameter distribution at fixed nvz
@@ -52,7 +60,7 @@ def surrogate_instances(n: int, seed: int, nz: int = 512, nvz: int = 128,
     return out
 
 
-def solve_pee(instances: list[Instance], chunk: int = 256, samples: int = 10,
+def solve_pee(instances: list[Instance], chunk: int = 256, samples: int = 20,
               tail: float = 0.2, stream=None) -> np.ndarray:
     """Ensemble-solver targets: P_ee(v) averaged over `samples` equally spaced
     times in the last `tail` of each run; returns [n][nvz]."""
@@ -162,12 +170,23 @@ class Surrogate:
     def __init__(self, n_models: int = 4, **mlp_kw):
         self.models = [MLP(seed=1000 + k, **mlp_kw) for k in range(n_models)]
 
-    def fit(self, x, t, **kw) -> list[np.ndarray]:
-        return [m.fit(x, t, seed=k + 1, **kw) for k, m in enumerate(self.models)]
+    def fit(self, x, t, epochs: int = 200, lr: float = 1e-3, schedule=(1.0, 0.3, 0.1),
+            **kw) -> list[np.ndarray]:
+        """AdamW in len(schedule) equal segments of the epochs with the
+        learning rate scaled by each factor (the optimizer state carries
+        over)."""
+        out = []
+        for k, m in enumerate(self.models):
+            seg = max(1, epochs // len(schedule))
+            out.append(np.concatenate([m.fit(x, t, epochs=seg, lr=lr * f, seed=k + 1 + 100 * j, **kw)
+                                       for j, f in enumerate(schedule)]))
+        return out
 
     def committee(self, x) -> tuple[np.ndarray, np.ndarray]:
+        """Committee mean and disagreement (RMS over v of the members' standard
+        deviation) per instance."""
         ys = np.stack([m.forward(x) for m in self.models])
-        return ys.mean(axis=0), ys.std(axis=0).max(axis=1)
+        return ys.mean(axis=0), np.sqrt((ys.std(axis=0) ** 2).mean(axis=1))
 
     def predict(self, instances: list[Instance], threshold: float = 1e-2,
                 solver=solve_pee) -> Prediction:

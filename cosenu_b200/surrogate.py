@@ -160,7 +160,7 @@ class MLP:
 @dataclass
 class Prediction:
     pee: np.ndarray          # [n][nvz] final answer
-    spread: np.ndarray       # [n] max over v of the committee's standard deviation
+    spread: np.ndarray       # [n] RMS over v of the committee's standard deviation
     fallback: np.ndarray     # [n] bool: solver used
 
 

@@ -27,7 +27,7 @@ EXPORTS = (
     "cosenu_time", "cosenu_analyse", "cosenu_pee_v", "cosenu_init_seeded",
     "cosenu_init_reference", "cosenu_device_state", "cosenu_upload_device",
     "cosenu_download_device", "cosenu_launches_per_step", "cosenu_tile", "cosenu_device_bytes",
-    "cosenu_step_noalloc",
+    "cosenu_step_noalloc", "cosenu_snapshot", "cosenu_snapshot_wait",
     "cosenu_batch_create", "cosenu_batch_destroy", "cosenu_batch_last_error",
     "cosenu_batch_size", "cosenu_batch_member", "cosenu_batch_init_seeded", "cosenu_batch_run",
     "cosenu_batch_synchronize", "cosenu_batch_autotune", "cosenu_batch_config",
@@ -107,6 +107,8 @@ def load(path: str | None = None) -> C.CDLL:
         "cosenu_tile": (i, [vp, C.POINTER(i), C.POINTER(i)]),
         "cosenu_device_bytes": (i, [vp, C.POINTER(C.c_size_t)]),
         "cosenu_step_noalloc": (i, [C.POINTER(Params), DPTR8, i, i, vp]),
+        "cosenu_snapshot": (i, [vp, C.POINTER(C.c_longlong)]),
+        "cosenu_snapshot_wait": (i, [vp, C.POINTER(C.POINTER(d))]),
         "cosenu_batch_create": (i, [i, C.POINTER(Params), C.POINTER(vp)]),
         "cosenu_batch_destroy": (i, [vp]),
         "cosenu_batch_last_error": (C.c_char_p, [vp]),

@@ -469,6 +469,14 @@ int cosenu_destroy(cosenu_ctx *ctx)
     for (void *b : bufs)
         if (b) cudaFree(b);
     if (ctx->h_pinned) cudaFreeHost(ctx->h_pinned);
+    if (ctx->snap_stream) {
+        cudaStreamSynchronize(ctx->snap_stream);
+        cudaStreamDestroy(ctx->snap_stream);
+    }
+    if (ctx->snap_taken) cudaEventDestroy(ctx->snap_taken);
+    if (ctx->snap_done) cudaEventDestroy(ctx->snap_done);
+    if (ctx->snap_d) cudaFree(ctx->snap_d);
+    if (ctx->snap_h) cudaFreeHost(ctx->snap_h);
     if (ctx->own_stream) cudaStreamDestroy(ctx->own_stream);
     delete ctx;
     return COSENU_OK;
@@ -555,6 +563,48 @@ int cosenu_download(cosenu_ctx *ctx, double *const comp[8], int gz)
     }
     CK(cudaStreamSynchronize(ctx->stream));
     return check_err_flag(ctx);
+}
+
+int cosenu_snapshot(cosenu_ctx *ctx, long long *steps)
+{
+    if (!ctx) return COSENU_ERR_ARG;
+    if (!ctx->have_state) return fail(ctx, COSENU_ERR_STATE, "no state uploaded");
+    if (ctx->next_stage != 0) return fail(ctx, COSENU_ERR_STATE, "RK4 step in progress");
+    DeviceGuard dg(ctx->p.device);
+    const int nz = ctx->p.nz, nvz = ctx->p.nvz;
+    const size_t n = (size_t)NCOMP * nvz * nz;
+    if (!ctx->snap_d) {
+        CK(cudaMalloc(&ctx->snap_d, n * sizeof(double)));
+        CK(cudaMallocHost(&ctx->snap_h, n * sizeof(double)));
+        CK(cudaStreamCreateWithFlags(&ctx->snap_stream, cudaStreamNonBlocking));
+        CK(cudaEventCreateWithFlags(&ctx->snap_taken, cudaEventDisableTiming));
+        CK(cudaEventCreateWithFlags(&ctx->snap_done, cudaEventDisableTiming));
+    }
+    // the previous host copy must be out of the device buffer before it is
+    // overwritten (ordered on the device; the caller is done with the host
+    // buffer by contract)
+    if (ctx->snap_pending) CK(cudaStreamWaitEvent(ctx->stream, ctx->snap_done, 0));
+    for (int c = 0; c < NCOMP; ++c)
+        CK(cudaMemcpy2DAsync(ctx->snap_d + (size_t)c * nvz * nz, (size_t)nz * 8,
+                             ctx->Y + (long long)c * ctx->cs + HP, (size_t)ctx->ld * 8,
+                             (size_t)nz * 8, nvz, cudaMemcpyDeviceToDevice, ctx->stream));
+    CK(cudaEventRecord(ctx->snap_taken, ctx->stream));
+    CK(cudaStreamWaitEvent(ctx->snap_stream, ctx->snap_taken, 0));
+    CK(cudaMemcpyAsync(ctx->snap_h, ctx->snap_d, n * sizeof(double), cudaMemcpyDeviceToHost,
+                       ctx->snap_stream));
+    CK(cudaEventRecord(ctx->snap_done, ctx->snap_stream));
+    ctx->snap_pending = true;
+    if (steps) *steps = ctx->steps;
+    return COSENU_OK;
+}
+
+int cosenu_snapshot_wait(cosenu_ctx *ctx, const double **data)
+{
+    if (!ctx || !data || !ctx->snap_pending) return COSENU_ERR_ARG;
+    DeviceGuard dg(ctx->p.device);
+    if (cudaEventSynchronize(ctx->snap_done) != cudaSuccess) return COSENU_ERR_CUDA;
+    *data = ctx->snap_h;
+    return COSENU_OK;
 }
 
 int cosenu_download_device(cosenu_ctx *ctx, double *const comp[8], int ld)

@@ -64,6 +64,12 @@ struct cosenu_ctx {
     int next_stage = 0;
     long long steps = 0;
     int mom_nvt_cap = 1;  // v tiles the moment buffers have room for
+    // snapshot: device copy of the interior state, its pinned host copy, the
+    // stream of the device-to-host copy and the events ordering the two
+    double *snap_d = nullptr, *snap_h = nullptr;
+    cudaStream_t snap_stream = nullptr;
+    cudaEvent_t snap_taken = nullptr, snap_done = nullptr;
+    bool snap_pending = false;
     std::string err;
 };
 

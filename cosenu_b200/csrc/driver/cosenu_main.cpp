@@ -126,14 +126,15 @@ int main(int argc, char *argv[])
                 state.analyse(t_iter, d);
                 state.surv_prob(t_iter, d);
             }
-            if (t_iter % pars.dump_interval == 0) state.dump_rho(t_iter);
-            if (checkpoint_every > 0 && t_iter % checkpoint_every == 0) state.write_state(t_iter);
+            state.write_output(t_iter, t_iter % pars.dump_interval == 0,
+                               checkpoint_every > 0 && t_iter % checkpoint_every == 0);
             if (t_iter % progress == 0)
                 std::cout << " " << std::setprecision(4)
                           << (int)(t_iter * 100.0 / (N_ITER - 1)) << " %" << std::endl;
             ++t_iter;
         }
         cosenu_synchronize(state.ctx());
+        state.finish_output();
         auto end = std::chrono::steady_clock::now();
         std::chrono::duration<double> el = end - start;
         std::cout << " 100 %" << std::endl << std::endl << "SIMULATION COMPLETED" << std::endl;

@@ -139,6 +139,21 @@ class NuOsc:
 
     v_stat = property(download)
 
+    def snapshot(self) -> int:
+        """Starts an asynchronous copy of the current state to pinned host
+        memory (cosenu_snapshot); returns the step count it was taken at."""
+        n = C.c_longlong()
+        self._check(self.lib.cosenu_snapshot(self.h, C.byref(n)))
+        return n.value
+
+    def snapshot_wait(self) -> np.ndarray:
+        """Waits for the last snapshot and returns a copy of it as [8][nvz][nz]
+        (interior cells)."""
+        p = C.POINTER(C.c_double)()
+        self._check(self.lib.cosenu_snapshot_wait(self.h, C.byref(p)))
+        n = 8 * self.nvz * self.nz
+        return np.ctypeslib.as_array(p, shape=(n,)).reshape(8, self.nvz, self.nz).copy()
+
     def set_profile(self, G: np.ndarray, bG: np.ndarray) -> None:
         G = self._host(G, 1)
         bG = self._host(bG, 1)

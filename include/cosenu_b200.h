@@ -192,6 +192,24 @@ int cosenu_device_state(cosenu_ctx *ctx, double *comp[8], int *ld);
 int cosenu_upload_device(cosenu_ctx *ctx, const double *const comp[8], int ld);
 int cosenu_download_device(cosenu_ctx *ctx, double *const comp[8], int ld);
 
+/* Snapshots for output written while stepping continues.  The reference's
+ * dump_rho and write_state (src/snaps.hpp:6-39,187-218) read the state on the
+ * host at the dump step, which stops the run for the whole file write.
+ * cosenu_snapshot queues on the context's stream a device copy of the current
+ * state (taken before any later step touches it), then, on a second stream,
+ * its copy to pinned host memory, and returns at once; *steps (if not NULL)
+ * receives the number of RK4 steps the snapshot is taken after.
+ * cosenu_snapshot_wait blocks until that host copy is complete and stores in
+ * *data the interior cells: 8 components of nvz rows of nz doubles, cell
+ * (v, z) of component c at data[((size_t)c * nvz + v) * nz + z].  The data
+ * stay valid until the next cosenu_snapshot or cosenu_destroy.
+ * cosenu_snapshot_wait touches only the snapshot's own buffers and events and
+ * sets no error text, so it may be called from another host thread while this
+ * one keeps stepping.  The two buffers (device and pinned host, 64 * nz * nvz
+ * bytes each) are allocated by the first cosenu_snapshot. */
+int cosenu_snapshot(cosenu_ctx *ctx, long long *steps);
+int cosenu_snapshot_wait(cosenu_ctx *ctx, const double **data);
+
 /* ---------------------------------------------------------------------------
  * Ensembles (no counterpart in the reference, which runs one configuration per
  * process: manage.py:361-428 submits one job per (nz, nvz, CFL)).  Many

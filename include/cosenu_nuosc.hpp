@@ -11,7 +11,9 @@
 //                 initialize / read_G0 / read_state / read_state0 /
 //                 write_state / write_state0 / step_rk4 / analyse /
 //                 surv_prob / dump_rho with the reference's file formats
-//                 (src/snaps.hpp, src/analysis.hpp).
+//                 (src/snaps.hpp, src/analysis.hpp).  rho_<t>.dat and the
+//                 state.bin checkpoint are written from a device snapshot by
+//                 a host thread while the GPU keeps stepping.
 #pragma once
 
 #include <cmath>
@@ -23,9 +25,11 @@
 #include <sstream>
 #include <stdexcept>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "cosenu_b200.h"
+#include "cosenu_format.hpp"
 
 namespace cosenu {
 
@@ -210,7 +214,11 @@ class NuOscGPU {
         G.assign(size, 0.0);
         bG.assign(size, 0.0);
     }
-    ~NuOscGPU() { cosenu_destroy(ctx_); }
+    ~NuOscGPU()
+    {
+        if (writer_.joinable()) writer_.join();
+        cosenu_destroy(ctx_);
+    }
     NuOscGPU(const NuOscGPU &) = delete;
     NuOscGPU &operator=(const NuOscGPU &) = delete;
 
@@ -248,19 +256,11 @@ class NuOscGPU {
 
     // -- binary files (src/snaps.hpp) ---------------------------------------
     // write_state: int32 iteration then 8 interleaved doubles per cell,
-    // written to state<t>.bin and renamed to state.bin (:6-39).
-    void write_state(unsigned int t)
-    {
-        download_state();
-        std::string tmp = "state" + std::to_string(t) + ".bin";
-        {
-            std::ofstream f(tmp, std::ios::out | std::ios::binary);
-            if (!f) throw Error(COSENU_ERR_ARG, "cannot open " + tmp);
-            f.write((const char *)&t, sizeof(int));
-            write_cells(f, v_stat);
-        }
-        std::rename(tmp.c_str(), "state.bin");
-    }
+    // written to state<t>.bin and renamed to state.bin (:6-39).  `t` is the
+    // iteration just completed; the header holds t + 1, the iteration a run
+    // resumed from the file (read_state) starts at -- the meaning state0.bin
+    // has with its implied t = 1 -- so a resumed run repeats no step.
+    void write_state(unsigned int t) { write_output(t, false, true); }
     void write_state0()
     {
         std::ofstream f("state0.bin", std::ios::out | std::ios::binary);
@@ -353,24 +353,44 @@ class NuOscGPU {
         o << t << "\t" << std::scientific << d.Pee << "\t" << d.Pbee << std::endl;
     }
     // NuOsc::dump_rho (src/snaps.hpp:187-218): rho_<t>.dat, z outer, v inner.
-    void dump_rho(unsigned int t)
+    void dump_rho(unsigned int t) { write_output(t, true, false); }
+
+    // rho_<t>.dat (rho) and/or the state.bin checkpoint (state) of the current
+    // state, from one snapshot: the device copies the state aside and the file
+    // is formatted and written by a host thread while stepping continues.
+    // Waits for the previous output first (its host buffer is reused).
+    void write_output(unsigned int t, bool rho, bool state)
     {
-        download_state();
-        std::string fn = "rho_" + std::to_string(t) + ".dat";
-        std::ofstream o(fn, std::ofstream::out | std::ofstream::trunc);
-        if (!o) {
-            std::cout << "Unable to open " << fn << "\n";
-            return;
-        }
-        const double *s = v_stat.data();
-        for (int j = 0; j < nz; ++j) {
-            for (int i = 0; i < nvz; ++i) {
-                size_t ij = idx(i, j);
-                o << Z[j] << "\t" << vz[i] << "\t" << std::setprecision(16);
-                for (int k = 0; k < NC; ++k)
-                    o << s[(size_t)k * size + ij] << (k + 1 < NC ? "\t" : "\n");
+        if (!rho && !state) return;
+        finish_output();
+        check(cosenu_snapshot(ctx_, nullptr));
+        writer_ = std::thread([this, t, rho, state] {
+            const double *d = nullptr;
+            if (cosenu_snapshot_wait(ctx_, &d) != COSENU_OK) {
+                writer_err_ = "snapshot copy to the host failed";
+                return;
             }
-            o << "\n";
+            const double *comp[NC];
+            for (int k = 0; k < NC; ++k) comp[k] = d + (size_t)k * nvz * nz;
+            if (rho) {
+                const std::string fn = "rho_" + std::to_string(t) + ".dat";
+                if (!format_rho(fn, nz, nvz, Z.data(), vz.data(), comp, nz))
+                    writer_msg_ += "Unable to open " + fn + "\n";
+            }
+            if (state && !write_state_file(t + 1, comp))
+                writer_err_ = "cannot write state" + std::to_string(t + 1) + ".bin";
+        });
+    }
+    // Waits for the output thread; throws if it failed to write a checkpoint.
+    void finish_output()
+    {
+        if (writer_.joinable()) writer_.join();
+        if (!writer_msg_.empty()) std::cout << writer_msg_;
+        writer_msg_.clear();
+        if (!writer_err_.empty()) {
+            std::string e;
+            e.swap(writer_err_);
+            throw Error(COSENU_ERR_ARG, e);
         }
     }
 
@@ -393,6 +413,27 @@ class NuOscGPU {
     void check(int rc)
     {
         if (rc != COSENU_OK) throw Error(rc, cosenu_last_error(ctx_));
+    }
+    std::thread writer_;
+    std::string writer_err_, writer_msg_;
+
+    // state.bin body (src/snaps.hpp:6-39): int32 iteration, then the 8
+    // components interleaved per cell, v-major; written to state<t>.bin and
+    // renamed into place.
+    bool write_state_file(unsigned int t, const double *const comp[NC])
+    {
+        const std::string tmp = "state" + std::to_string(t) + ".bin";
+        FILE *f = std::fopen(tmp.c_str(), "wb");
+        if (!f) return false;
+        bool ok = std::fwrite(&t, sizeof(int), 1, f) == 1;
+        std::vector<double> row((size_t)nz * NC);
+        for (int i = 0; i < nvz && ok; ++i) {
+            for (int j = 0; j < nz; ++j)
+                for (int k = 0; k < NC; ++k) row[(size_t)j * NC + k] = comp[k][(size_t)i * nz + j];
+            ok = std::fwrite(row.data(), sizeof(double), row.size(), f) == row.size();
+        }
+        ok = (std::fclose(f) == 0) && ok;
+        return ok && std::rename(tmp.c_str(), "state.bin") == 0;
     }
     void write_cells(std::ofstream &f, const std::vector<double> &s)
     {

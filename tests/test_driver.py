@@ -106,3 +106,37 @@ def test_driver_fresh_start_matches_reference(tmp_path):
     cq_got = open(tmp_path / "conserved_quantities.dat").read().splitlines()
     assert cq_got[0] == cq_ref[0]
     assert len(cq_got) == len(cq_ref)
+
+
+@pytest.mark.gpu
+def test_driver_checkpoint_and_resume(tmp_path, oracle):
+    """--checkpoint-every writes state.bin (src/snaps.hpp:6-39 format) from
+    the asynchronous device snapshot while stepping goes on; its header is
+    the next iteration to run, so a run resumed from it with --ff ends where
+    the uninterrupted reference run ends."""
+    import shutil
+    from oracle.oracle import read_rho_dat, read_state_bin
+    case, d = load_golden("fv_small")
+    n_iter, anal, ndump = int(d["n_iter"]), int(d["anal_every"]), int(d["n_dump_rho"])
+    a = tmp_path / "a"
+    a.mkdir()
+    _job(a, case, d, oracle, n_iter, anal, ndump)
+    p = subprocess.run([_driver(), "--conf", "job.config", "--ff", "--presets", "presets.hpp",
+                        "--checkpoint-every", "15"], cwd=a, capture_output=True, text=True,
+                       timeout=300)
+    assert p.returncode == 0, p.stdout + p.stderr
+    st, t = read_state_bin(str(a / "state.bin"), case, header=True)
+    assert t == 16
+    assert np.abs(st[:, :, case.gz:case.gz + case.nz] - d["rho_15"]).max() <= 1e-10
+    assert not any(f.startswith("state1") for f in os.listdir(a))  # renamed into place
+    b = tmp_path / "b"
+    b.mkdir()
+    for f in ("job.config", "G0.bin", "state0.bin", "presets.hpp", "state.bin"):
+        shutil.copy(a / f, b / f)
+    p = subprocess.run([_driver(), "--conf", "job.config", "--ff", "--presets", "presets.hpp"],
+                       cwd=b, capture_output=True, text=True, timeout=300)
+    assert p.returncode == 0, p.stdout + p.stderr
+    assert "Starting time = 16" in p.stdout
+    got = read_rho_dat(str(b / "rho_20.dat"), case)
+    assert np.abs(got - d["rho_20"]).max() <= 1e-10
+    assert not (b / "rho_15.dat").exists()

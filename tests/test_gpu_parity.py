@@ -114,6 +114,27 @@ def test_deterministic_and_graph_equals_stagewise(gpu_lib, oracle):
     assert np.array_equal(outs[0], outs[2])
 
 
+def test_snapshot_is_the_state_at_the_call(gpu_lib, oracle):
+    """cosenu_snapshot: the host copy holds the state at the call even when
+    more steps are queued before cosenu_snapshot_wait; consecutive snapshots
+    reuse the buffers."""
+    case, d = load_golden("fv_vac")
+    st0, _, _ = _inputs(case, d, oracle)
+    with gpu_from_case(case) as sim:
+        sim.upload(st0)
+        sim.evolve(5)
+        assert sim.snapshot() == 5
+        sim.evolve(11)
+        snap5 = sim.snapshot_wait()
+        ref16 = _interior(case, sim.download())
+        assert sim.snapshot() == 16
+        snap16 = sim.snapshot_wait()
+    ref5 = oracle.step(case, st0, 5)
+    assert np.array_equal(snap16, ref16)
+    assert maxabs_per_comp(snap5, _interior(case, ref5)).max() <= 1e-10
+    assert not np.array_equal(snap5, snap16)
+
+
 def test_device_initial_conditions_bitwise(gpu_lib, oracle):
     """On-device seeded and reference initial conditions equal the host
     recipes bit for bit."""

@@ -153,7 +153,8 @@ int run_phase(cosenu_batch *b, const std::vector<int> &active, long long nsteps)
     std::vector<int> ranges;
     size_t ntiles_all = 0;
     for (int i : active) ntiles_all += b->m[i]->p.nz / 32;
-    const int nblk = (int)std::min<size_t>(std::max<size_t>(ntiles_all, 1), (size_t)b->nsm);
+    const int per_sm = b->use_tma ? tma_blocks_per_sm(b->scheme) : 1;
+    const int nblk = (int)std::min<size_t>(std::max<size_t>(ntiles_all, 1), (size_t)(per_sm * b->nsm));
     size_t nt = build_table(b, active, tab, &ranges, nblk);
     if (nt == 0 || nsteps <= 0) return COSENU_OK;
     // table entries, then (TMA family) the nblk + 1 block range starts

@@ -136,6 +136,8 @@ StageArgs stage_args(const cosenu_ctx *ctx, int stage)
     a.ko_order = ctx->p.ko_order;
     a.dt = ctx->dt;
     a.dv = ctx->dv;
+    a.v0 = ctx->p.v0;
+    a.dz = ctx->dz;
     a.mu = ctx->p.mu;
     a.ct = ctx->ct;
     a.st = ctx->st;
@@ -158,7 +160,8 @@ cudaError_t launch_stage(cosenu_ctx *ctx, int stage, cudaStream_t s)
     StageArgs a = stage_args(ctx, stage);
     if (ctx->use_tma) {
         const CUtensorMap &mX = stage == 1 ? ctx->mY40 : (stage == 3 ? ctx->mU1_40 : ctx->mU0_40);
-        int nblk = std::min(ctx->p.nz / tma_box_tile(), ctx->nsm);
+        int nblk = std::min(ctx->p.nz / tma_box_tile(),
+                            tma_blocks_per_sm(ctx->p.scheme) * ctx->nsm);
         return launch_rk4_stage_tma(mX, ctx->mY32, ctx->mA32, a, ctx->p.scheme, stage, ctx->fp32,
                                     ctx->err_flag, nblk, s);
     }

@@ -42,6 +42,7 @@ struct StageArgs {
     int H;               // ghost cells written per side
     int bc, flags, fd_advec, ko_order;
     double dt, dv, mu, ct, st, pmo, ko_eps;
+    double v0, dz;       // velocity grid origin, cell width (rows recompute vz)
 };
 
 // Ensemble launch: one stage launch covers every active instance.  Entry t of

@@ -22,6 +22,7 @@ int make_state_map(CUtensorMap *map, const void *base, int elem_bytes, int ld, i
 int tma_box_x();
 int tma_box_tile();
 int tma_max_nvz();
+int tma_blocks_per_sm(int scheme);
 cudaError_t tma_prepare();
 cudaError_t launch_rk4_stage_tma(const CUtensorMap &mX, const CUtensorMap &mY,
                                  const CUtensorMap &mA, const StageArgs &a, int scheme, int stage,

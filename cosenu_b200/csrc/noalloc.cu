@@ -200,6 +200,8 @@ extern "C" int cosenu_step_noalloc(const cosenu_params *pp, double *const state[
     a.ko_order = p.ko_order;
     a.dt = p.cfl * dz;
     a.dv = dv;
+    a.v0 = p.v0;
+    a.dz = dz;
     a.mu = p.mu;
     const double th = p.theta_deg * M_PI / 180.0;
     a.ct = (1.0 / 2.0) * p.omega * cos(2.0 * th);

@@ -11,7 +11,11 @@
 // their stencil from shared memory and write the results with coalesced
 // stores.  Full/empty mbarriers order the ring.  With up to NBUF-1 chunks in
 // flight (~100 KB per SM) the kernel keeps HBM busy without depending on
-// occupancy, which the register-heavy FP64 right-hand side limits.
+// occupancy, which the register-heavy FP64 right-hand side limits.  FD runs
+// one block per SM; FV, bound by FP64 issue rather than HBM, runs two (each
+// with half the shared memory and <= 112 registers per thread) so that twice
+// the warps hide the latency of the WENO7 arithmetic.  Per-row velocities and
+// advection factors are recomputed in registers, bit-equal to the host tables.
 //
 // FV: a warp holds one row, so every lane reconstructs the upwind WENO7 face it
 // owns from the shared-memory stencil and takes its neighbour's face by
@@ -139,8 +143,27 @@ __device__ __forceinline__ void tma_tile(const BatchDev &bd, int t, int &inst, i
     }
 }
 
-template <int SCHEME, bool GEN, int STAGE, class TC, class TIN, class TOUT, int NBUF, bool BATCHED>
-__global__ void __launch_bounds__(tma::NTHR, 1)
+// Velocity and advection factor of row i, recomputed with round-to-nearest
+// operations so the bits equal the host tables (capi.cu, src/nuosc.hpp:88-92,
+// rhs_fv.hpp:145, rhs_fd.hpp:57): no per-row table occupies shared memory.
+template <int SCHEME>
+__device__ __forceinline__ void row_values(const StageArgs &a, int i, double &v, double &f)
+{
+    v = __dadd_rn(a.v0, __dmul_rn(__dadd_rn((double)i, 0.5), a.dv));
+    if (SCHEME == FV) {
+        f = __ddiv_rn(-v, a.dz);
+    } else {
+        const double sv = (double)((0.0 < v) - (v < 0.0));
+        const double d12 = __dmul_rn(12.0, a.dz);
+        if (a.fd_advec == 0) f = __ddiv_rn(-v, d12);          // centre
+        else if (a.fd_advec == 1) f = __ddiv_rn(__dmul_rn(-sv, v), d12);  // upwind
+        else f = __ddiv_rn(__dmul_rn(sv, v), d12);                       // lopsided
+    }
+}
+
+template <int SCHEME, bool GEN, int STAGE, class TC, class TIN, class TOUT, int NBUF, bool BATCHED,
+          int MINB>
+__global__ void __launch_bounds__(tma::NTHR, MINB)
     rk4_stage_tma_kernel(const __grid_constant__ CUtensorMap mX,
                          const __grid_constant__ CUtensorMap mY,
                          const __grid_constant__ CUtensorMap mA,
@@ -151,10 +174,8 @@ __global__ void __launch_bounds__(tma::NTHR, 1)
     extern __shared__ __align__(1024) unsigned char smem[];
     uint64_t *full = reinterpret_cast<uint64_t *>(smem + NBUF * L::BUF);
     uint64_t *empty = full + NBUF;
-    double(*s_mom)[NMOM][TZ] = reinterpret_cast<double(*)[NMOM][TZ]>(empty + NBUF);
-    double(*s_red)[NMOM][TZ] = s_mom + 2;                   // [R/2][6][TZ]
-    double *s_vz = reinterpret_cast<double *>(s_red + R / 2);  // [tab] velocities
-    double *s_fac = s_vz + bd.tab;                             // [tab] advection factors
+    double(*s_mom)[TZ] = reinterpret_cast<double(*)[TZ]>(empty + NBUF);  // [6][TZ]
+    double(*s_red)[NMOM][TZ] = reinterpret_cast<double(*)[NMOM][TZ]>(s_mom + NMOM);  // [R/2]
 
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const int nzt = BATCHED ? bd.ntiles : a0.nz / TZ;
@@ -202,43 +223,26 @@ __global__ void __launch_bounds__(tma::NTHR, 1)
     }
 
     // ---------------------------------------------------------------- consumers
-    if (!BATCHED)
-        for (int i = tid; i < a0.nvz; i += NCONS) {
-            s_vz[i] = a0.vz[i];
-            s_fac[i] = a0.rowfac[i];
-        }
     // this block's tiles: a contiguous range of the ensemble table, or every
     // gridDim.x-th z tile of a single simulation
     const int t_first = BATCHED ? bd.range[blockIdx.x] : blockIdx.x;
     const int t_end = BATCHED ? bd.range[blockIdx.x + 1] : nzt;
     const int t_step = BATCHED ? 1 : gridDim.x;
     // moments of the stage input for the first tile
-    int k = 0;
     if (t_first < t_end && tid < NMOM * TZ) {
         int inst, zt;
         tma_tile<BATCHED>(bd, t_first, inst, zt);
         const StageArgs &a = BATCHED ? bd.args[inst * 4 + STAGE - 1] : a0;
         if (a.flags & F_COLL)
-            s_mom[0][tid / TZ][tid % TZ] = a.Min[(long long)(tid / TZ) * a.nz + zt * TZ + tid % TZ];
+            s_mom[tid / TZ][tid % TZ] = a.Min[(long long)(tid / TZ) * a.nz + zt * TZ + tid % TZ];
     }
     consumer_sync();
 
     uint32_t it = 0;
-    int prev_inst = -1;
-    for (int t = t_first; t < t_end; t += t_step, ++k) {
+    for (int t = t_first; t < t_end; t += t_step) {
         int inst, zt;
         tma_tile<BATCHED>(bd, t, inst, zt);
         const StageArgs &a = BATCHED ? bd.args[inst * 4 + STAGE - 1] : a0;
-        if (BATCHED && inst != prev_inst) {
-            // per-row tables of this instance
-            consumer_sync();
-            for (int i = tid; i < a.nvz; i += NCONS) {
-                s_vz[i] = a.vz[i];
-                s_fac[i] = a.rowfac[i];
-            }
-            consumer_sync();
-            prev_inst = inst;
-        }
         const int nch = (a.nvz + R - 1) / R;
         const bool coll = (a.flags & F_COLL) != 0;
         const bool advec = (a.flags & F_ADVEC_OFF) == 0;
@@ -248,7 +252,6 @@ __global__ void __launch_bounds__(tma::NTHR, 1)
         const TC ko_eps = (TC)a.ko_eps;
         const int z0 = zt * TZ;
         const int z = z0 + lane;
-        const int cur = k & 1;
         // prefetch the next tile's input moments into a register
         double mnext = 0.0;
         const int tn = t + t_step;
@@ -260,9 +263,8 @@ __global__ void __launch_bounds__(tma::NTHR, 1)
                 mnext = an.Min[(long long)(tid / TZ) * an.nz + zn * TZ + tid % TZ];
         }
         double macc[NMOM] = {0, 0, 0, 0, 0, 0};
-        const double M0A = s_mom[cur][0][lane], M0B = s_mom[cur][1][lane],
-                     M0C = s_mom[cur][2][lane], M1A = s_mom[cur][3][lane],
-                     M1B = s_mom[cur][4][lane], M1C = s_mom[cur][5][lane];
+        const double M0A = s_mom[0][lane], M0B = s_mom[1][lane], M0C = s_mom[2][lane],
+                     M1A = s_mom[3][lane], M1B = s_mom[4][lane], M1C = s_mom[5][lane];
         const TC hm = (a.flags & F_MAT) ? (TC)a.Hm[z] : TC(0);
 
         for (int ch = 0; ch < nch; ++ch, ++it) {
@@ -270,8 +272,9 @@ __global__ void __launch_bounds__(tma::NTHR, 1)
             const int v = ch * R + warp;
             const bool valid = v < a.nvz;
             const int vr = valid ? v : a.nvz - 1;
-            const double vzv = s_vz[vr];
-            const TC factor = (TC)s_fac[vr];
+            double vzv, fac;
+            row_values<SCHEME>(a, vr, vzv, fac);
+            const TC factor = (TC)fac;
             tma::mbar_wait(&full[b], (it / NBUF) & 1, err, 2);
             const unsigned char *buf = smem + b * L::BUF;
             const TIN *xrow = reinterpret_cast<const TIN *>(buf) + warp * XW + HALO;
@@ -488,7 +491,7 @@ __global__ void __launch_bounds__(tma::NTHR, 1)
 #pragma unroll
                 for (int w = 0; w < R / 2; ++w) s += s_red[w][m][zz];
                 if (coll) a.Mout[(long long)m * a.nz + z0 + zz] = s;
-                s_mom[cur ^ 1][m][zz] = mnext;
+                s_mom[m][zz] = mnext;  // every consumer read this tile's values above
             }
             consumer_sync();
         }
@@ -541,82 +544,125 @@ int tma_box_tile() { return tma::TZ; }
 int tma_max_nvz() { return TMA_MAX_NVZ; }
 
 static const int TMA_SMEM_MAX = 232448;  // opt-in shared memory per block on sm_100
+static const int TMA_SMEM_SM = 233472;   // shared memory per SM (1 KB reserved per block)
 
-// Shared memory of one block with an NB-deep ring and per-row tables for
-// `tab` rows.
+// Shared memory of one block with an NB-deep ring.
 template <class TIN, int STAGE>
-static int tma_smem(int NB, int tab)
+static int tma_smem(int NB)
 {
     using L = tma::Layout<TIN, STAGE>;
-    return NB * L::BUF + 2 * NB * 8 + (2 + tma::R / 2) * NMOM * tma::TZ * 8 + 2 * tab * 8;
+    return NB * L::BUF + 2 * NB * 8 + (1 + tma::R / 2) * NMOM * tma::TZ * 8;
 }
 
-template <int SCHEME, bool GEN, int STAGE, class TC, class TIN, class TOUT, int NB>
+static int tma_smem_limit(int minb)
+{
+    return minb == 1 ? TMA_SMEM_MAX : TMA_SMEM_SM / minb - 1024;
+}
+
+template <int SCHEME, bool GEN, int STAGE, class TC, class TIN, class TOUT, int NB, int MINB>
 static cudaError_t launch_nb(const CUtensorMap &mX, const CUtensorMap &mY, const CUtensorMap &mA,
                              const StageArgs &a, int *err, int nblocks, cudaStream_t s,
-                             const BatchDev *bd, int tab)
+                             const BatchDev *bd)
 {
-    auto kern = rk4_stage_tma_kernel<SCHEME, GEN, STAGE, TC, TIN, TOUT, NB, false>;
-    auto kernb = rk4_stage_tma_kernel<SCHEME, GEN, STAGE, TC, TIN, TOUT, NB, true>;
-    if (nblocks <= 0) {  // preparation call: raise the dynamic shared-memory limit
-        cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                             TMA_SMEM_MAX);
-        if (e != cudaSuccess) return e;
-        return cudaFuncSetAttribute(kernb, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                    TMA_SMEM_MAX);
+    auto kern = rk4_stage_tma_kernel<SCHEME, GEN, STAGE, TC, TIN, TOUT, NB, false, MINB>;
+    auto kernb = rk4_stage_tma_kernel<SCHEME, GEN, STAGE, TC, TIN, TOUT, NB, true, MINB>;
+    if (nblocks <= 0) {  // preparation call: shared-memory limit and carveout
+        for (auto k : {kern, kernb}) {
+            cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                 TMA_SMEM_MAX);
+            if (e == cudaSuccess)
+                e = cudaFuncSetAttribute(k, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                         (int)cudaSharedmemCarveoutMaxShared);
+            if (e != cudaSuccess) return e;
+        }
+        return cudaSuccess;
     }
-    const int shmem = tma_smem<TIN, STAGE>(NB, tab);
-    if (bd) {
-        BatchDev b2 = *bd;
-        b2.tab = tab;
-        kernb<<<nblocks, tma::NTHR, shmem, s>>>(mX, mY, mA, a, err, b2);
-    } else {
-        BatchDev b2{};
-        b2.tab = tab;
-        kern<<<nblocks, tma::NTHR, shmem, s>>>(mX, mY, mA, a, err, b2);
-    }
+    const int shmem = tma_smem<TIN, STAGE>(NB);
+    if (bd)
+        kernb<<<nblocks, tma::NTHR, shmem, s>>>(mX, mY, mA, a, err, *bd);
+    else
+        kern<<<nblocks, tma::NTHR, shmem, s>>>(mX, mY, mA, a, err, BatchDev{});
     return cudaGetLastError();
 }
 
-// A 4-deep ring where it fits in shared memory (always, except FP64 stages 2
-// and 3 with more than ~600 rows), else 3-deep.
+// Ring depth of the FD FP64 stages 2-3 (three 53 KB operand sets per chunk):
+// 3 buffers measured faster than 4 at nz 32768 x nvz 256 (0.525 vs 0.545 ms
+// per stage); COSENU_TMA_RING=4 selects the 4-deep ring where it fits.
+static int tma_ring_env()
+{
+    static int v = -1;
+    if (v < 0) {
+        const char *e = getenv("COSENU_TMA_RING");
+        v = (e && e[0] == '4') ? 4 : 3;
+    }
+    return v;
+}
+
+// Blocks per SM.  FD (memory bound): one, with the deepest ring that fits.
+// FV (FP64 bound, 9 warps per block): two, to hide FP64 and shared-memory
+// latency with twice the warps, each with the deepest ring that fits in half
+// the SM (COSENU_TMA_MINB=1 selects one block per SM with a 4-deep ring).
+static int tma_minb_env()
+{
+    static int v = -1;
+    if (v < 0) {
+        const char *e = getenv("COSENU_TMA_MINB");
+        v = (e && e[0] == '1') ? 1 : 2;
+    }
+    return v;
+}
+
+int tma_blocks_per_sm(int scheme) { return scheme == FV ? tma_minb_env() : 1; }
+
 template <int SCHEME, bool GEN, int STAGE, class TC, class TIN, class TOUT>
 static cudaError_t launch_one(const CUtensorMap &mX, const CUtensorMap &mY, const CUtensorMap &mA,
                               const StageArgs &a, int *err, int nblocks, cudaStream_t s,
-                              const BatchDev *bd, int max_nvz)
+                              const BatchDev *bd)
 {
-    constexpr bool MAY_NEED_3 = (STAGE == 2 || STAGE == 3) && sizeof(TIN) == 8;
-    const int tab = (max_nvz + 7) / 8 * 8;
-    if (nblocks <= 0) {
-        cudaError_t e = launch_nb<SCHEME, GEN, STAGE, TC, TIN, TOUT, 4>(mX, mY, mA, a, err, 0, s, bd, tab);
-        if (e != cudaSuccess || !MAY_NEED_3) return e;
-        return launch_nb<SCHEME, GEN, STAGE, TC, TIN, TOUT, MAY_NEED_3 ? 3 : 4>(mX, mY, mA, a, err, 0,
-                                                                               s, bd, tab);
+#define LNB(NB, MINB) \
+    launch_nb<SCHEME, GEN, STAGE, TC, TIN, TOUT, NB, MINB>(mX, mY, mA, a, err, nblocks, s, bd)
+    if (SCHEME == FD) {
+        if (nblocks <= 0) {
+            cudaError_t e = LNB(4, 1);
+            return e == cudaSuccess ? LNB(3, 1) : e;
+        }
+        const bool cap3 = (STAGE == 2 || STAGE == 3) && sizeof(TIN) == 8 && tma_ring_env() == 3;
+        if (tma_smem<TIN, STAGE>(4) <= tma_smem_limit(1) && !cap3) return LNB(4, 1);
+        return LNB(3, 1);
     }
-    if (tma_smem<TIN, STAGE>(4, tab) <= TMA_SMEM_MAX || !MAY_NEED_3)
-        return launch_nb<SCHEME, GEN, STAGE, TC, TIN, TOUT, 4>(mX, mY, mA, a, err, nblocks, s, bd, tab);
-    return launch_nb<SCHEME, GEN, STAGE, TC, TIN, TOUT, MAY_NEED_3 ? 3 : 4>(mX, mY, mA, a, err,
-                                                                           nblocks, s, bd, tab);
+    if (nblocks <= 0) {
+        cudaError_t e = LNB(4, 1);
+        if (e == cudaSuccess) e = LNB(4, 2);
+        if (e == cudaSuccess) e = LNB(3, 2);
+        if (e == cudaSuccess) e = LNB(2, 2);
+        return e;
+    }
+    if (tma_minb_env() == 1) return LNB(4, 1);
+    const int lim = tma_smem_limit(2);
+    if (tma_smem<TIN, STAGE>(4) <= lim) return LNB(4, 2);
+    if (tma_smem<TIN, STAGE>(3) <= lim) return LNB(3, 2);
+    return LNB(2, 2);
+#undef LNB
 }
 
 template <int SCHEME, bool GEN>
 static cudaError_t launch_p(const CUtensorMap &mX, const CUtensorMap &mY, const CUtensorMap &mA,
                             const StageArgs &a, int stage, int fp32, int *err, int nblocks,
-                            cudaStream_t s, const BatchDev *bd, int max_nvz)
+                            cudaStream_t s, const BatchDev *bd)
 {
     if (fp32) {
         switch (stage) {
-        case 1: return launch_one<SCHEME, GEN, 1, float, double, float>(mX, mY, mA, a, err, nblocks, s, bd, max_nvz);
-        case 2: return launch_one<SCHEME, GEN, 2, float, float, float>(mX, mY, mA, a, err, nblocks, s, bd, max_nvz);
-        case 3: return launch_one<SCHEME, GEN, 3, float, float, float>(mX, mY, mA, a, err, nblocks, s, bd, max_nvz);
-        case 4: return launch_one<SCHEME, GEN, 4, float, float, double>(mX, mY, mA, a, err, nblocks, s, bd, max_nvz);
+        case 1: return launch_one<SCHEME, GEN, 1, float, double, float>(mX, mY, mA, a, err, nblocks, s, bd);
+        case 2: return launch_one<SCHEME, GEN, 2, float, float, float>(mX, mY, mA, a, err, nblocks, s, bd);
+        case 3: return launch_one<SCHEME, GEN, 3, float, float, float>(mX, mY, mA, a, err, nblocks, s, bd);
+        case 4: return launch_one<SCHEME, GEN, 4, float, float, double>(mX, mY, mA, a, err, nblocks, s, bd);
         }
     } else {
         switch (stage) {
-        case 1: return launch_one<SCHEME, GEN, 1, double, double, double>(mX, mY, mA, a, err, nblocks, s, bd, max_nvz);
-        case 2: return launch_one<SCHEME, GEN, 2, double, double, double>(mX, mY, mA, a, err, nblocks, s, bd, max_nvz);
-        case 3: return launch_one<SCHEME, GEN, 3, double, double, double>(mX, mY, mA, a, err, nblocks, s, bd, max_nvz);
-        case 4: return launch_one<SCHEME, GEN, 4, double, double, double>(mX, mY, mA, a, err, nblocks, s, bd, max_nvz);
+        case 1: return launch_one<SCHEME, GEN, 1, double, double, double>(mX, mY, mA, a, err, nblocks, s, bd);
+        case 2: return launch_one<SCHEME, GEN, 2, double, double, double>(mX, mY, mA, a, err, nblocks, s, bd);
+        case 3: return launch_one<SCHEME, GEN, 3, double, double, double>(mX, mY, mA, a, err, nblocks, s, bd);
+        case 4: return launch_one<SCHEME, GEN, 4, double, double, double>(mX, mY, mA, a, err, nblocks, s, bd);
         }
     }
     return cudaErrorInvalidValue;
@@ -627,10 +673,10 @@ cudaError_t launch_rk4_stage_tma(const CUtensorMap &mX, const CUtensorMap &mY,
                                  int fp32, int *err, int nblocks, cudaStream_t s)
 {
     if (scheme == FV)
-        return launch_p<FV, false>(mX, mY, mA, a, stage, fp32, err, nblocks, s, nullptr, a.nvz);
+        return launch_p<FV, false>(mX, mY, mA, a, stage, fp32, err, nblocks, s, nullptr);
     const bool gen = a.fd_advec != 0 || a.ko_order == 5;
-    return gen ? launch_p<FD, true>(mX, mY, mA, a, stage, fp32, err, nblocks, s, nullptr, a.nvz)
-               : launch_p<FD, false>(mX, mY, mA, a, stage, fp32, err, nblocks, s, nullptr, a.nvz);
+    return gen ? launch_p<FD, true>(mX, mY, mA, a, stage, fp32, err, nblocks, s, nullptr)
+               : launch_p<FD, false>(mX, mY, mA, a, stage, fp32, err, nblocks, s, nullptr);
 }
 
 // Ensemble launch: `a` carries the variant switches shared by every instance
@@ -641,10 +687,10 @@ cudaError_t launch_rk4_stage_tma_batch(const BatchDev &bd, const StageArgs &a, i
 {
     CUtensorMap m{};
     if (scheme == FV)
-        return launch_p<FV, false>(m, m, m, a, stage, fp32, err, nblocks, s, &bd, max_nvz);
+        return launch_p<FV, false>(m, m, m, a, stage, fp32, err, nblocks, s, &bd);
     const bool gen = a.fd_advec != 0 || a.ko_order == 5;
-    return gen ? launch_p<FD, true>(m, m, m, a, stage, fp32, err, nblocks, s, &bd, max_nvz)
-               : launch_p<FD, false>(m, m, m, a, stage, fp32, err, nblocks, s, &bd, max_nvz);
+    return gen ? launch_p<FD, true>(m, m, m, a, stage, fp32, err, nblocks, s, &bd)
+               : launch_p<FD, false>(m, m, m, a, stage, fp32, err, nblocks, s, &bd);
 }
 
 // Sets the shared-memory attribute of every instantiation on the current device.

@@ -585,17 +585,33 @@ static cudaError_t launch_nb(const CUtensorMap &mX, const CUtensorMap &mY, const
     return cudaGetLastError();
 }
 
-// Ring depth of the FD FP64 stages 2-3 (three 53 KB operand sets per chunk):
-// 3 buffers measured faster than 4 at nz 32768 x nvz 256 (0.525 vs 0.545 ms
-// per stage); COSENU_TMA_RING=4 selects the 4-deep ring where it fits.
+// Ring depth of the FD kernel (one block per SM): the deepest ring of at most
+// 4 buffers that total at most ~112 KB.  Measured at nz 32768 x nvz 256, more
+// bytes in flight per SM lower the achieved HBM bandwidth (FP64 stages 2-3,
+// 53 KB per chunk: 0.441 / 0.534 / 0.545 ms per stage with 2 / 3 / 4 buffers;
+// FP64 stage 4, 37 KB: 3 buffers best; FP32 stages 2-3, 43 KB: 2 best; FP64
+// stage 1, 20 KB: 4 buffers 0.318 ms, 5 buffers 0.344 ms).
+// COSENU_TMA_RING=n (2..4) overrides the depth where it fits.
 static int tma_ring_env()
 {
     static int v = -1;
     if (v < 0) {
         const char *e = getenv("COSENU_TMA_RING");
-        v = (e && e[0] == '4') ? 4 : 3;
+        v = (e && e[0] >= '2' && e[0] <= '4' && e[1] == 0) ? e[0] - '0' : 0;
     }
     return v;
+}
+
+template <class TIN, int STAGE>
+static int tma_fd_ring()
+{
+    using L = tma::Layout<TIN, STAGE>;
+    int nb = 2;
+    while (nb < 4 && (nb + 1) * L::BUF <= 112 * 1024) ++nb;
+    const int e = tma_ring_env();
+    if (e) nb = e;
+    while (nb > 2 && tma_smem<TIN, STAGE>(nb) > tma_smem_limit(1)) --nb;
+    return nb;
 }
 
 // Blocks per SM.  FD (memory bound): one, with the deepest ring that fits.
@@ -621,27 +637,32 @@ static cudaError_t launch_one(const CUtensorMap &mX, const CUtensorMap &mY, cons
 {
 #define LNB(NB, MINB) \
     launch_nb<SCHEME, GEN, STAGE, TC, TIN, TOUT, NB, MINB>(mX, mY, mA, a, err, nblocks, s, bd)
-    if (SCHEME == FD) {
+    if constexpr (SCHEME == FD) {
+        if (nblocks <= 0) {
+            cudaError_t e = LNB(2, 1);
+            if (e == cudaSuccess) e = LNB(3, 1);
+            if (e == cudaSuccess) e = LNB(4, 1);
+            return e;
+        }
+        switch (tma_fd_ring<TIN, STAGE>()) {
+        case 2: return LNB(2, 1);
+        case 3: return LNB(3, 1);
+        default: return LNB(4, 1);
+        }
+    } else {
         if (nblocks <= 0) {
             cudaError_t e = LNB(4, 1);
-            return e == cudaSuccess ? LNB(3, 1) : e;
+            if (e == cudaSuccess) e = LNB(4, 2);
+            if (e == cudaSuccess) e = LNB(3, 2);
+            if (e == cudaSuccess) e = LNB(2, 2);
+            return e;
         }
-        const bool cap3 = (STAGE == 2 || STAGE == 3) && sizeof(TIN) == 8 && tma_ring_env() == 3;
-        if (tma_smem<TIN, STAGE>(4) <= tma_smem_limit(1) && !cap3) return LNB(4, 1);
-        return LNB(3, 1);
+        if (tma_minb_env() == 1) return LNB(4, 1);
+        const int lim = tma_smem_limit(2);
+        if (tma_smem<TIN, STAGE>(4) <= lim) return LNB(4, 2);
+        if (tma_smem<TIN, STAGE>(3) <= lim) return LNB(3, 2);
+        return LNB(2, 2);
     }
-    if (nblocks <= 0) {
-        cudaError_t e = LNB(4, 1);
-        if (e == cudaSuccess) e = LNB(4, 2);
-        if (e == cudaSuccess) e = LNB(3, 2);
-        if (e == cudaSuccess) e = LNB(2, 2);
-        return e;
-    }
-    if (tma_minb_env() == 1) return LNB(4, 1);
-    const int lim = tma_smem_limit(2);
-    if (tma_smem<TIN, STAGE>(4) <= lim) return LNB(4, 2);
-    if (tma_smem<TIN, STAGE>(3) <= lim) return LNB(3, 2);
-    return LNB(2, 2);
 #undef LNB
 }
 

@@ -31,6 +31,8 @@
 // built from six per-z moments.  Each block writes its per-v-tile partial
 // moments; the consumer sums the partials in a fixed order, so results are
 // bitwise reproducible run to run.
+#include <type_traits>
+
 #include "common.cuh"
 #include "weno.cuh"
 
@@ -361,8 +363,11 @@ static cudaError_t launch_t(const StageArgs &a, int stage, cudaStream_t s, const
 {
     dim3 grid = B ? dim3(bd.ntiles) : dim3(a.nz / TZ, a.nvt), block(NTHREADS);
     if (grid.x == 0) return cudaSuccess;
+    // FP32-bulk FD stage 1 keeps FP64 arithmetic: its input is the FP64 state
+    // and narrowing the 5-point stencil costs more issue than FP64 saves
+    using TC1 = std::conditional_t<SCHEME == FD, double, TC>;
     switch (stage) {
-    case 1: rk4_stage_kernel<SCHEME, 1, TZ, TC, TIN1, TU, B><<<grid, block, 0, s>>>(a, bd); break;
+    case 1: rk4_stage_kernel<SCHEME, 1, TZ, TC1, TIN1, TU, B><<<grid, block, 0, s>>>(a, bd); break;
     case 2: rk4_stage_kernel<SCHEME, 2, TZ, TC, TU, TU, B><<<grid, block, 0, s>>>(a, bd); break;
     case 3: rk4_stage_kernel<SCHEME, 3, TZ, TC, TU, TU, B><<<grid, block, 0, s>>>(a, bd); break;
     case 4: rk4_stage_kernel<SCHEME, 4, TZ, TC, TU, double, B><<<grid, block, 0, s>>>(a, bd); break;

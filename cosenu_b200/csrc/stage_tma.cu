@@ -29,6 +29,8 @@
 // left waiting and the host reports the error.
 #include <cuda.h>
 
+#include <type_traits>
+
 #include "common.cuh"
 #include "weno.cuh"
 
@@ -673,7 +675,9 @@ static cudaError_t launch_p(const CUtensorMap &mX, const CUtensorMap &mY, const 
 {
     if (fp32) {
         switch (stage) {
-        case 1: return launch_one<SCHEME, GEN, 1, float, double, float>(mX, mY, mA, a, err, nblocks, s, bd);
+        // FD stage 1 keeps FP64 arithmetic on its FP64 input (see stage.cu)
+        case 1: return launch_one<SCHEME, GEN, 1, std::conditional_t<SCHEME == FD, double, float>,
+                                  double, float>(mX, mY, mA, a, err, nblocks, s, bd);
         case 2: return launch_one<SCHEME, GEN, 2, float, float, float>(mX, mY, mA, a, err, nblocks, s, bd);
         case 3: return launch_one<SCHEME, GEN, 3, float, float, float>(mX, mY, mA, a, err, nblocks, s, bd);
         case 4: return launch_one<SCHEME, GEN, 4, float, float, double>(mX, mY, mA, a, err, nblocks, s, bd);

@@ -40,8 +40,8 @@ sys.path.insert(0, ROOT)
 
 METRIC = "cell-updates/s (nz*nvz*RK4 steps), FP64"
 UNIT = "cell-updates/s"
-# FD at scale (the headline); configs[0]: FV WENO7 small; configs[2]:
-# FV at 65536 x 512 (FP32-bulk form, FP64 for comparison)
+# c2: FD at scale (the headline); c1: FV WENO7 on the small 1024 x 64 grid; c3: FV
+# at 65536 x 512 (FP32-bulk form, FP64 for comparison)
 WORKLOADS = {
     "c2": dict(nz=32768, nvz=256, gz=2, z0=-3000.0, z1=3000.0, v0=-1.0, v1=1.0, cfl=0.4,
                pmo=1.0, omega=1e-3, theta_deg=1e-6, mu=1.0, scheme="fd"),
@@ -385,7 +385,7 @@ def run_reference_arm(args):
 
 
 def run_ensemble(args):
-    """256 uneven FV instances to t = 1000/mu in one ensemble
+    """The ensemble workload: 256 uneven FV instances to t = 1000/mu in one ensemble
     (autotuned kernel family and tiles), against the plain single-instance
     FP64 path timed on a stratified subset (every 8th instance, full step
     counts) and scaled by work."""
@@ -443,7 +443,7 @@ def run_ensemble(args):
     t_plain = t_sub * sum(work) / w_sub
     n = len(xs)
     print(json.dumps({
-        "metric": "instances/s (configs[3] ensemble to t = 1000/mu)", "value": n / t_batch,
+        "metric": "instances/s (256-instance FV ensemble to t = 1000/mu)", "value": n / t_batch,
         "unit": "instances/s", "n_gpus": 1, "instances": n,
         "cell_updates_per_s": sum(work) / t_batch, "seconds": t_batch,
         "plain_fp64_instances_per_s": n / t_plain,
@@ -459,7 +459,7 @@ def run_ensemble(args):
 
 
 def run_fp32_study(args):
-    """the FP32-bulk form against the FP64 form on the same seeded
+    """FV at 65536 x 512: the FP32-bulk form against the FP64 form on the same seeded
     input: max-abs error per component at the end, <Pee>(t) error, trace and
     ELN drift of both, and the throughput of each (timed separately)."""
     import numpy as np
@@ -519,7 +519,8 @@ def run_fp32_study(args):
 
 
 def run_surrogate(args):
-    """configs[4] (reduced): solver targets for a training and a
+    """The surrogate workload (nz fixed at 512 to fit the training set in
+    the run time): solver targets for a training and a
     held-out set, a committee of networks trained on the GPU, held-out error
     against the solver with and without the disagreement fallback, and the
     time of both routes."""

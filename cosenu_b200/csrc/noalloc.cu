@@ -44,8 +44,8 @@ cudaError_t launch_moments(const double *X, double *M, const double *vz, long lo
 using namespace cosenu;
 
 // Capacity: nvz * ld_padded <= NOALLOC_MAX_PLANE cells per component plane
-// (ld_padded = nz + 32 rounded up to a multiple of 16; the configs[0] grid,
-// 1024 x 64, needs 67 584) and nz <= NOALLOC_MAX_NZ.
+// (ld_padded = nz + 32 rounded up to a multiple of 16; the 1024 x 64 FV
+// grid needs 67 584) and nz <= NOALLOC_MAX_NZ.
 #define NOALLOC_MAX_PLANE 69632
 #define NOALLOC_MAX_NZ 16384
 #define NOALLOC_MAX_NVZ 4096

@@ -1,6 +1,6 @@
 """Ensembles of independent simulations advanced together on one GPU
-(cosenu_batch_* of include/cosenu_b200.h), and the configs[3] instance
-distribution.
+(cosenu_batch_* of include/cosenu_b200.h), and the distribution of the
+256-instance FV ensemble workload.
 
 The reference runs one configuration per process (manage.py:361-428 submits
 one job per (nz, nvz, CFL)); here hundreds of uneven instances share every
@@ -52,7 +52,7 @@ def steps_to(t_end: float, nz: int, z0: float = -600.0, z1: float = 600.0,
 
 def ensemble_instances(n: int = 256, seed: int = 20240601, t_factor: float = 1000.0,
                        nvz_choices=(32, 64, 128, 256), nz_range=(512, 8192)) -> list[Instance]:
-    """nz log-uniform in [512, 8192] rounded to 256, nvz from
+    """The ensemble workload: nz log-uniform in [512, 8192] rounded to 256, nvz from
     {32, 64, 128, 256}, alpha ~ U[0.6, 1.2], sigma_nu ~ U[0.4, 0.8],
     sigma_nubar ~ U[0.3, 0.7], mu ~ U[0.5, 2], its own seeded +-1e-6 ex
     perturbation, run to t = t_factor / mu on z in [-600, 600]."""

@@ -47,8 +47,9 @@ def reseeded(instances: list[Instance], offset: int = 7919) -> list[Instance]:
 
 def surrogate_instances(n: int, seed: int, nz: int = 512, nvz: int = 128,
                         t_factor: float = 1000.0) -> list[Instance]:
-    """configs[4] inputs: the configs[3] parameter distribution at fixed nvz
-    (and, to fit the training set in budget, fixed nz)."""
+    """Surrogate inputs: the ensemble parameter distribution
+    (ensemble.ensemble_instances) at fixed nvz (and, to keep the training
+    set affordable, fixed nz)."""
     rng = np.random.default_rng(seed)
     out = []
     for i in range(n):

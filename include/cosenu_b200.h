@@ -277,7 +277,7 @@ int cosenu_mlp_train(cosenu_mlp *net, int epochs, int batch, float lr, float wei
  * Working memory is one fixed device array inside the library (20.5 MB, held by
  * every GPU that loads the library until exit): grids need
  * nvz * (nz + 32 rounded up to a multiple of 16) <= 69632 and nz <= 16384
- * (the configs[0] grid, 1024 x 64, fits); larger grids return COSENU_ERR_ARG
+ * (the 1024 x 64 grid fits); larger grids return COSENU_ERR_ARG
  * with the limit in cosenu_last_error(NULL).  The first call on a device looks
  * up that array's address; make it before any stream capture.  Calls share the
  * array, so calls whose GPU work overlaps race; order them.  Work is queued on

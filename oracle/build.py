@@ -1,4 +1,4 @@
-"""Build recipe for the checker side (test infrastructure only).
+"""Build recipe for the oracle side (test infrastructure only).
 
 1. ``oracle/libcosenu_oracle.so`` -- the plain-C restatement in
    ``cosenu_oracle.c`` (gcc, -O3, no FMA contraction, no fast-math, so its

@@ -1,7 +1,7 @@
 /*
  * cosenu_oracle.c -- CPU restatement of COSEnu's RK4 time-stepping path.
  *
- * TEST INFRASTRUCTURE ONLY.  This file is the checker that the CUDA path is
+ * TEST INFRASTRUCTURE ONLY.  This file is the oracle that the CUDA path is
  * compared against; it is imported only by tests/, by __graft_entry__.smoke()
  * and by bench.py's cpu_baseline leg.  Nothing in the product links it.
  *

@@ -1,4 +1,4 @@
-"""Python handle on the checker (test infrastructure only).
+"""Python handle on the oracle (test infrastructure only).
 
 * ``Oracle`` -- ctypes wrapper of ``libcosenu_oracle.so`` (the C restatement
   in ``cosenu_oracle.c``), working on numpy arrays in the reference layout

@@ -41,14 +41,14 @@ SEED = 20240601
 # itself then produces NaN).
 SB = dict(z0=-32.0, z1=32.0)
 CASES = {
-    # configs[0] physics (FV, omega = 0, mu = 1) on a small grid
+    # the small FV workload's physics (omega = 0, mu = 1) on a small grid
     "fv_small": (dict(nz=64, nvz=16, gz=4, scheme="fv", omega=0.0, **SB), 21, 5, 4, False),
     # FV with a vacuum term (cosenu_configs.yaml defaults: omega 1e-2, theta 37 deg)
     "fv_vac": (dict(nz=64, nvz=16, gz=4, scheme="fv", omega=1e-2, theta_deg=37.0, **SB), 21, 5, 4, False),
     # odd nvz puts a v = 0 row on the grid (sign(v) = 0 branch of rhs_fv.hpp:147-162)
     "fv_oddv": (dict(nz=32, nvz=15, gz=4, scheme="fv", omega=1e-2, theta_deg=37.0, z0=-16.0,
                       z1=16.0), 11, 5, 2, False),
-    # configs[1] physics (FD, omega 1e-3, theta 1e-6 deg, NO) on a small grid
+    # the large FD workload's physics (omega 1e-3, theta 1e-6 deg, NO) on a small grid
     "fd_small": (dict(nz=64, nvz=16, gz=2, scheme="fd", omega=1e-3, theta_deg=1e-6, **SB), 21, 5, 4, False),
     "fd_vac": (dict(nz=64, nvz=16, gz=2, scheme="fd", omega=1e-2, theta_deg=37.0, pmo=-1.0, **SB),
                21, 5, 4, False),
@@ -66,9 +66,9 @@ CASES = {
                        theta_deg=37.0, **SB), 11, 5, 2, False),
     "fd_advoff": (dict(nz=64, nvz=16, gz=2, scheme="fd", advec_off=True, omega=1e-2,
                        theta_deg=37.0, **SB), 11, 5, 2, False),
-    # configs[0] exactly: FV, nz 1024, nvz 64, 500 steps (pre-saturation)
+    # the small FV workload exactly: nz 1024, nvz 64, 500 steps (pre-saturation)
     "c1_pre": (dict(nz=1024, nvz=64, gz=4, scheme="fv", omega=0.0), 501, 50, 2, True),
-    # the configs[0] grid run through saturation (<Pee> leaves 1 near step 350)
+    # the 1024 x 64 FV grid run through saturation (<Pee> leaves 1 near step 350)
     "c1_sat": (dict(nz=1024, nvz=64, gz=4, scheme="fv", omega=0.0), 1501, 25, 3, True),
 }
 

@@ -158,7 +158,7 @@ def _c1(oracle, name):
 
 
 def test_c1_pre_saturation_500_steps(gpu_lib, oracle):
-    """configs[0] as specified (FV WENO7, 1024 x 64, 500 steps): against the
+    """The small FV workload as specified (WENO7, 1024 x 64, 500 steps): against the
     reference run (subset, checksums, analysis rows) and the full oracle
     state, <= 1e-10 max-abs per component."""
     case, d, G, bG, st0 = _c1(oracle, "c1_pre")
@@ -187,7 +187,7 @@ def test_c1_pre_saturation_500_steps(gpu_lib, oracle):
 
 
 def test_c1_after_saturation_1500_steps(gpu_lib, oracle):
-    """The configs[0] grid through saturation: <Pee>, <Pbee>, |M0|, max dP and
+    """The 1024 x 64 FV grid through saturation: <Pee>, <Pbee>, |M0|, max dP and
     P_ee(v) against the reference run at every analysis step, <= 1e-6."""
     case, d, G, bG, st0 = _c1(oracle, "c1_sat")
     worst = 0.0
@@ -210,7 +210,7 @@ def test_c1_after_saturation_1500_steps(gpu_lib, oracle):
 
 
 def test_c2_full_size_one_step_and_conservation(gpu_lib, oracle):
-    """configs[1] grid (FD, 32768 x 256): one step at full size against the
+    """The large FD grid (32768 x 256): one step at full size against the
     oracle, then trace conservation over further steps."""
     from oracle.oracle import Case
     case = Case(nz=32768, nvz=256, gz=2, z0=-3000.0, z1=3000.0, scheme="fd", pmo=1.0,

@@ -116,7 +116,7 @@ def _c1_run(oracle, name, nthreads=0):
 
 
 def test_oracle_c1_pre_saturation(oracle):
-    """configs[0] as specified: FV 1024 x 64, 500 steps; subset, checksums and
+    """The small FV workload as specified: 1024 x 64, 500 steps; subset, checksums and
     the analysis rows of the reference run."""
     case, d, G, bG, st0 = _c1_run(oracle, "c1_pre")
     y, t_prev = st0, 0
@@ -136,7 +136,7 @@ def test_oracle_c1_pre_saturation(oracle):
 
 @pytest.mark.slow
 def test_oracle_c1_after_saturation(oracle):
-    """The configs[0] grid through saturation (1500 steps): survival
+    """The 1024 x 64 FV grid through saturation (1500 steps): survival
     probabilities and |M0| rows of the reference, <= 1e-6."""
     case, d, G, bG, st0 = _c1_run(oracle, "c1_sat")
     y, t_prev = st0, 0

@@ -1,4 +1,4 @@
-"""Learned surrogate end to end on a reduced configs[4] set: targets from the
+"""Learned surrogate end to end on a reduced surrogate set: targets from the
 ensemble solver, a committee trained on the GPU, held-out error against the
 solver, what the trained network gains over predicting without it, and the
 disagreement fallback."""
@@ -12,7 +12,7 @@ pytestmark = pytest.mark.gpu
 
 def test_surrogate_pipeline_reduced(gpu_lib):
     from cosenu_b200.surrogate import Surrogate, features, solve_pee, surrogate_instances
-    # reduced: nz 256 on [-600, 600], runs to t = 250 / mu, nvz 128 as configs[4]
+    # reduced: nz 256 on [-600, 600], runs to t = 250 / mu, nvz 128 as the full surrogate workload
     train = surrogate_instances(192, seed=11, nz=256, t_factor=250.0)
     test = surrogate_instances(48, seed=12, nz=256, t_factor=250.0)
     t0 = time.perf_counter()

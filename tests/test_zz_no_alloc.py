@@ -32,7 +32,7 @@ def _call(p, dev, nz, nsteps):
 
 @pytest.mark.gpu
 @pytest.mark.parametrize("kw", [
-    dict(scheme="fv", nz=1024, nvz=64, gz=4, omega=0.0),                # the configs[0] grid
+    dict(scheme="fv", nz=1024, nvz=64, gz=4, omega=0.0),                # the small FV grid
     dict(scheme="fd", nz=512, nvz=48, gz=2, omega=1e-3, theta_deg=1e-6, z0=-256.0, z1=256.0),
     dict(scheme="fv", nz=256, nvz=20, gz=4, bc="open", omega=1e-2, theta_deg=37.0, z0=-128.0,
          z1=128.0),

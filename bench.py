@@ -547,7 +547,7 @@ def run_surrogate(args):
     x_test = np.stack([features(i) for i in test])
     sur = Surrogate(n_models=4)
     t0 = time.perf_counter()
-    losses = sur.fit(x_train, y_train, epochs=args.epochs, batch=256, lr=1e-3)
+    losses = sur.fit(x_train, y_train, epochs=args.epochs, batch=64, lr=2e-3)
     t_fit = time.perf_counter() - t0
     sur.committee(x_test[:8])  # warm-up
     t0 = time.perf_counter()
@@ -586,10 +586,10 @@ def main():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--instances", type=int, default=256, help="c4: ensemble size")
-    ap.add_argument("--train", type=int, default=2048, help="c5: training instances")
+    ap.add_argument("--train", type=int, default=4096, help="c5: training instances")
     ap.add_argument("--test", type=int, default=512, help="c5: held-out instances")
     ap.add_argument("--sur-nz", type=int, default=512, help="c5: nz of the solver runs")
-    ap.add_argument("--epochs", type=int, default=900, help="c5: training epochs")
+    ap.add_argument("--epochs", type=int, default=300, help="c5: training epochs")
     ap.add_argument("--threshold", type=float, default=1e-2, help="c5: fallback threshold")
     ap.add_argument("--fp32-study", action="store_true",
                     help="FP32-bulk vs FP64 error study on the chosen workload")

@@ -215,6 +215,16 @@ __global__ void gather_kernel(const float *X, const float *T, const int *idx, in
 }  // namespace
 
 // ---------------------------------------------------------------------------
+// eacc += sum of the nb per-block partial losses (fixed order).
+__global__ void loss_accumulate_kernel(const float *partial, int nb, double *eacc)
+{
+    if (threadIdx.x == 0) {
+        double s = 0.0;
+        for (int i = 0; i < nb; ++i) s += partial[i];
+        *eacc += s;
+    }
+}
+
 struct cosenu_mlp {
     int nin = 0, kpad = 0, nh = 0, nl = 0, nout = 0, device = 0;
     std::vector<int> din, dout;      // per layer
@@ -229,7 +239,8 @@ struct cosenu_mlp {
     std::vector<__nv_bfloat16 *> Hb;  // activations [cap][dout]
     float *dA = nullptr, *dB = nullptr;
     __nv_bfloat16 *dAb = nullptr;
-    float *T = nullptr, *partial = nullptr;
+    float *T = nullptr, *partial = nullptr;  // partial: 1024 floats, then eacc
+    double *eacc = nullptr;                   // epoch loss sum, on the device
     // resident training data
     float *dX = nullptr, *dT = nullptr;
     int *didx = nullptr;
@@ -373,10 +384,11 @@ int cosenu_mlp_create(int n_in, int n_hidden, int n_hidden_layers, int n_out, ui
         cudaMalloc(&net->m1, net->nparam * 4) != cudaSuccess ||
         cudaMalloc(&net->m2, net->nparam * 4) != cudaSuccess ||
         cudaMalloc(&net->wb, net->nparam * 2) != cudaSuccess ||
-        cudaMalloc(&net->partial, 1024 * 4) != cudaSuccess) {
+        cudaMalloc(&net->partial, 1024 * 4 + 8) != cudaSuccess) {
         cosenu_mlp_destroy(net);
         return COSENU_ERR_NOMEM;
     }
+    net->eacc = reinterpret_cast<double *>(net->partial + 1024);
     *out = net;
     return cosenu_mlp_set_params(net, h.data());
 }
@@ -513,7 +525,7 @@ int cosenu_mlp_train(cosenu_mlp *net, int epochs, int batch, float lr, float wei
     std::vector<int> perm(net->ndata);
     uint64_t st = shuffle_seed * 6364136223846793005ull + 1442695040888963407ull;
     const int nb = 32;
-    std::vector<float> part(nb);
+    double esum = 0;
     for (int e = 0; e < epochs; ++e) {
         for (int i = 0; i < net->ndata; ++i) perm[i] = i;
         for (int i = net->ndata - 1; i > 0; --i) {  // Fisher-Yates
@@ -523,7 +535,7 @@ int cosenu_mlp_train(cosenu_mlp *net, int epochs, int batch, float lr, float wei
         }
         MCK(cudaMemcpyAsync(net->didx, perm.data(), (size_t)net->ndata * 4, cudaMemcpyHostToDevice,
                             net->stream));
-        double esum = 0;
+        MCK(cudaMemsetAsync(net->eacc, 0, sizeof(double), net->stream));
         long long ecount = 0;
         for (int b0 = 0; b0 < net->ndata; b0 += batch) {
             const int rows = std::min(batch, net->ndata - b0);
@@ -546,11 +558,12 @@ int cosenu_mlp_train(cosenu_mlp *net, int epochs, int batch, float lr, float wei
                     net->m2 + net->boff[l], net->wb + net->boff[l], net->dout[l], lr, beta1, beta2,
                     eps, 0.f, c1, c2);
             }
-            MCK(cudaMemcpyAsync(part.data(), net->partial, nb * 4, cudaMemcpyDeviceToHost, net->stream));
-            MCK(cudaStreamSynchronize(net->stream));
-            for (float p : part) esum += p;
+            loss_accumulate_kernel<<<1, 32, 0, net->stream>>>(net->partial, nb, net->eacc);
             ecount += (long long)rows * net->nout;
         }
+        // one host synchronisation per epoch (the shuffle buffer is reused)
+        MCK(cudaMemcpyAsync(&esum, net->eacc, sizeof(double), cudaMemcpyDeviceToHost, net->stream));
+        MCK(cudaStreamSynchronize(net->stream));
         if (epoch_loss) epoch_loss[e] = (float)(esum / ecount);
     }
     MCK(cudaGetLastError());

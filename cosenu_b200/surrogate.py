@@ -146,16 +146,25 @@ class MLP:
                                                   x.shape[0], C.byref(loss), g.ctypes.data))
         return loss.value, g
 
-    def fit(self, x: np.ndarray, t: np.ndarray, epochs: int = 200, batch: int = 256,
-            lr: float = 1e-3, weight_decay: float = 1e-4, seed: int = 0) -> np.ndarray:
+    def set_data(self, x: np.ndarray, t: np.ndarray) -> None:
+        """Training set, held on the device for train()."""
         x = np.ascontiguousarray(x, dtype=np.float32)
         t = np.ascontiguousarray(t, dtype=np.float32)
         self._check(self.lib.cosenu_mlp_set_data(self.h, x.ctypes.data, t.ctypes.data,
                                                  x.shape[0]))
+
+    def train(self, epochs: int = 200, batch: int = 256, lr: float = 1e-3,
+              weight_decay: float = 1e-4, seed: int = 0) -> np.ndarray:
+        """AdamW epochs over the data of set_data(); returns each epoch's mean loss."""
         losses = np.zeros(epochs, dtype=np.float32)
         self._check(self.lib.cosenu_mlp_train(self.h, epochs, batch, lr, weight_decay, 0.9, 0.999,
                                               1e-8, seed, losses.ctypes.data))
         return losses
+
+    def fit(self, x: np.ndarray, t: np.ndarray, epochs: int = 200, batch: int = 256,
+            lr: float = 1e-3, weight_decay: float = 1e-4, seed: int = 0) -> np.ndarray:
+        self.set_data(x, t)
+        return self.train(epochs, batch, lr, weight_decay, seed)
 
 
 @dataclass
@@ -166,27 +175,47 @@ class Prediction:
 
 
 class Surrogate:
-    """Committee of networks with solver fallback."""
+    """Committee of networks with solver fallback.  Inputs are standardised
+    per feature with the training set's mean and spread."""
 
     def __init__(self, n_models: int = 4, **mlp_kw):
         self.models = [MLP(seed=1000 + k, **mlp_kw) for k in range(n_models)]
+        self.x_mean = None
+        self.x_std = None
 
-    def fit(self, x, t, epochs: int = 200, lr: float = 1e-3, schedule=(1.0, 0.3, 0.1),
+    def _norm(self, x) -> np.ndarray:
+        x = np.asarray(x, dtype=np.float64)
+        if self.x_mean is None:
+            return x.astype(np.float32)
+        return ((x - self.x_mean) / self.x_std).astype(np.float32)
+
+    def fit(self, x, t, epochs: int = 300, lr: float = 2e-3, schedule="cos",
             **kw) -> list[np.ndarray]:
-        """AdamW in len(schedule) equal segments of the epochs with the
-        learning rate scaled by each factor (the optimizer state carries
-        over)."""
+        """AdamW from the library's training kernels.  schedule "cos": the
+        learning rate follows lr * (1 + cos(pi e / epochs)) / 2 over the epochs;
+        a tuple of factors: equal segments of the epochs at lr * factor.  The
+        optimizer state carries over between epochs and segments."""
+        x = np.asarray(x, dtype=np.float64)
+        self.x_mean = x.mean(axis=0)
+        self.x_std = x.std(axis=0) + 1e-6
+        xn = self._norm(x)
+        if schedule == "cos":
+            plan = [(1, 0.5 * (1.0 + math.cos(math.pi * e / epochs))) for e in range(epochs)]
+        else:
+            seg = max(1, epochs // len(schedule))
+            plan = [(seg, f) for f in schedule]
         out = []
         for k, m in enumerate(self.models):
-            seg = max(1, epochs // len(schedule))
-            out.append(np.concatenate([m.fit(x, t, epochs=seg, lr=lr * f, seed=k + 1 + 100 * j, **kw)
-                                       for j, f in enumerate(schedule)]))
+            m.set_data(xn, t)
+            out.append(np.concatenate([m.train(epochs=n, lr=lr * f, seed=k + 1 + 100 * j, **kw)
+                                       for j, (n, f) in enumerate(plan)]))
         return out
 
     def committee(self, x) -> tuple[np.ndarray, np.ndarray]:
         """Committee mean and disagreement (RMS over v of the members' standard
         deviation) per instance."""
-        ys = np.stack([m.forward(x) for m in self.models])
+        xn = self._norm(x)
+        ys = np.stack([m.forward(xn) for m in self.models])
         return ys.mean(axis=0), np.sqrt((ys.std(axis=0) ** 2).mean(axis=1))
 
     def predict(self, instances: list[Instance], threshold: float = 1e-2,

@@ -357,15 +357,17 @@ def run_reference_arm(args):
         return
     threads = os.cpu_count() or 1
     nvz = WORKLOAD["nvz"]
-    # size the z-subset so that warm-up + K steps take about two minutes
-    t, n = _ref_run(64, 9, threads)
-    per_cell_step = t / (64 * nvz * n)
+    # size the z-subset so that warm-up + K steps take about 90 s (the
+    # reference driver needs N_ITER >= 10, i.e. at least 9 steps per run)
+    t, n = _ref_run(512, 9, threads)
+    per_cell_step = t / (512 * nvz * n)
     K, W = max(args.steps, 9), args.warmup
+    W_run = max(W, 9) if W > 0 else 0
     nz = 64
-    while nz * 2 <= WORKLOAD["nz"] and per_cell_step * nz * 2 * nvz * (K + W) <= 120.0:
+    while nz * 2 <= WORKLOAD["nz"] and per_cell_step * nz * 2 * nvz * (K + W_run) <= 90.0:
         nz *= 2
-    if W > 0:
-        _ref_run(nz, max(W, 9), threads)
+    if W_run:
+        _ref_run(nz, W_run, threads)
     t, n = _ref_run(nz, K, threads)
     value = nz * nvz * n / t
     sample = (f"reference {WORKLOAD['scheme'].upper()} build (g++ -O3 -fopenmp, "

@@ -92,7 +92,7 @@ size_t build_table(cosenu_batch *b, const std::vector<int> &active, std::vector<
         for (int i : active) {
             const cosenu_params &p = b->m[i]->p;
             for (int zt = 0; zt < p.nz / 32; ++zt) {
-                out.push_back(make_int4(i, zt, 0, 0));
+                out.push_back(make_int4(i, zt, 0, p.nvz));  // .w: rows, read by the kernel
                 w.push_back((long long)(p.nvz + 7) / 8 + 1);  // chunks + per-tile overhead
             }
         }
@@ -170,6 +170,7 @@ int run_phase(cosenu_batch *b, const std::vector<int> &active, long long nsteps)
     BCK(cudaEventRecord(b->table_ev[k], b->stream));
     BatchDev bd{b->d_table[k], (int)nt, b->d_args, b->d_maps,
                 reinterpret_cast<const int *>(b->d_table[k] + nt)};
+    if (getenv("COSENU_BATCH_RR")) bd.range = nullptr;
     int max_nvz = 0;
     for (int i : active) max_nvz = std::max(max_nvz, b->m[i]->p.nvz);
     const StageArgs a0 = ctx_stage_args(b->m[active[0]], 1);

@@ -46,7 +46,7 @@ struct StageArgs {
 };
 
 // Ensemble launch: one stage launch covers every active instance.  Entry t of
-// `table` names (instance, z tile, v tile); `args` holds the four stage
+// `table` names (instance, z tile, v tile, rows: nvz in the TMA family); `args` holds the four stage
 // arguments of every instance and `maps` its five tensor maps (Y and U0/U1
 // input boxes, Y and A tile boxes).
 struct BatchDev {

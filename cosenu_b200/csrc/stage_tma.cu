@@ -118,6 +118,12 @@ __device__ __forceinline__ void tma_load_3d(void *dst, const CUtensorMap *map, i
         : "memory");
 }
 
+// Brings a tensor map held in global memory into the TMA unit's cache.
+__device__ __forceinline__ void prefetch_map(const CUtensorMap *map)
+{
+    asm volatile("prefetch.tensormap [%0];" ::"l"((uint64_t)map) : "memory");
+}
+
 __device__ __forceinline__ void consumer_sync()
 {
     asm volatile("bar.sync 1, %0;" ::"n"(NCONS) : "memory");
@@ -149,16 +155,17 @@ __device__ __forceinline__ void tma_tile(const BatchDev &bd, int t, int &inst, i
 // operations so the bits equal the host tables (capi.cu, src/nuosc.hpp:88-92,
 // rhs_fv.hpp:145, rhs_fd.hpp:57): no per-row table occupies shared memory.
 template <int SCHEME>
-__device__ __forceinline__ void row_values(const StageArgs &a, int i, double &v, double &f)
+__device__ __forceinline__ void row_values(double v0, double dv, double dz, int fd_advec, int i,
+                                           double &v, double &f)
 {
-    v = __dadd_rn(a.v0, __dmul_rn(__dadd_rn((double)i, 0.5), a.dv));
+    v = __dadd_rn(v0, __dmul_rn(__dadd_rn((double)i, 0.5), dv));
     if (SCHEME == FV) {
-        f = __ddiv_rn(-v, a.dz);
+        f = __ddiv_rn(-v, dz);
     } else {
         const double sv = (double)((0.0 < v) - (v < 0.0));
-        const double d12 = __dmul_rn(12.0, a.dz);
-        if (a.fd_advec == 0) f = __ddiv_rn(-v, d12);          // centre
-        else if (a.fd_advec == 1) f = __ddiv_rn(__dmul_rn(-sv, v), d12);  // upwind
+        const double d12 = __dmul_rn(12.0, dz);
+        if (fd_advec == 0) f = __ddiv_rn(-v, d12);          // centre
+        else if (fd_advec == 1) f = __ddiv_rn(__dmul_rn(-sv, v), d12);  // upwind
         else f = __ddiv_rn(__dmul_rn(sv, v), d12);                       // lopsided
     }
 }
@@ -195,20 +202,33 @@ __global__ void __launch_bounds__(tma::NTHR, MINB)
         // ------------------------------------------------------------ producer
         if (lane == 0) {
             uint32_t it = 0;
-            const int t_first = BATCHED ? bd.range[blockIdx.x] : blockIdx.x;
-            const int t_end = BATCHED ? bd.range[blockIdx.x + 1] : nzt;
-            const int t_step = BATCHED ? 1 : gridDim.x;
+            const bool rr = !BATCHED || bd.range == nullptr;  // interleaved tiles
+            const int t_first = rr ? blockIdx.x : bd.range[blockIdx.x];
+            const int t_end = rr ? nzt : bd.range[blockIdx.x + 1];
+            const int t_step = rr ? gridDim.x : 1;
+            // batched: table entries (member, z tile, -, nvz) are read one tile
+            // ahead, and a new member's tensor maps (global memory) are
+            // prefetched while the previous tile streams
+            int4 cur = make_int4(0, 0, 0, 0);
+            if (BATCHED && t_first < t_end) cur = bd.table[t_first];
             for (int t = t_first; t < t_end; t += t_step) {
-                int inst, zt;
-                tma_tile<BATCHED>(bd, t, inst, zt);
-                const StageArgs &a = BATCHED ? bd.args[inst * 4 + STAGE - 1] : a0;
+                const bool has_next = t + t_step < t_end;
+                int4 nxt = cur;
+                if (BATCHED && has_next) nxt = bd.table[t + t_step];
+                const int inst = BATCHED ? cur.x : 0, zt = BATCHED ? cur.y : t;
                 const CUtensorMap *px =
                     BATCHED ? &bd.maps[inst * 5 + (STAGE == 1 ? 0 : (STAGE == 3 ? 2 : 1))] : &mX;
                 const CUtensorMap *py = BATCHED ? &bd.maps[inst * 5 + 3] : &mY;
                 const CUtensorMap *pa = BATCHED ? &bd.maps[inst * 5 + 4] : &mA;
                 const int z0 = zt * TZ;
-                const int nch = (a.nvz + R - 1) / R;
+                const int nch = ((BATCHED ? cur.w : a0.nvz) + R - 1) / R;
                 for (int ch = 0; ch < nch; ++ch, ++it) {
+                    if (BATCHED && ch == 0 && has_next && nxt.x != inst) {
+                        const CUtensorMap *m = &bd.maps[nxt.x * 5];
+                        tma::prefetch_map(&m[STAGE == 1 ? 0 : (STAGE == 3 ? 2 : 1)]);
+                        if (L::YB) tma::prefetch_map(&m[3]);
+                        if (L::AB) tma::prefetch_map(&m[4]);
+                    }
                     const int b = it % NBUF;
                     if (it >= (uint32_t)NBUF)
                         tma::mbar_wait(&empty[b], ((it / NBUF) - 1) & 1, err, 1);
@@ -219,6 +239,7 @@ __global__ void __launch_bounds__(tma::NTHR, MINB)
                     if (L::AB)
                         tma::tma_load_3d(buf + L::XB + L::YB, pa, HP + z0, ch * R, 0, &full[b]);
                 }
+                cur = nxt;
             }
         }
         return;
@@ -227,9 +248,10 @@ __global__ void __launch_bounds__(tma::NTHR, MINB)
     // ---------------------------------------------------------------- consumers
     // this block's tiles: a contiguous range of the ensemble table, or every
     // gridDim.x-th z tile of a single simulation
-    const int t_first = BATCHED ? bd.range[blockIdx.x] : blockIdx.x;
-    const int t_end = BATCHED ? bd.range[blockIdx.x + 1] : nzt;
-    const int t_step = BATCHED ? 1 : gridDim.x;
+    const bool rr = !BATCHED || bd.range == nullptr;
+    const int t_first = rr ? blockIdx.x : bd.range[blockIdx.x];
+    const int t_end = rr ? nzt : bd.range[blockIdx.x + 1];
+    const int t_step = rr ? gridDim.x : 1;
     // moments of the stage input for the first tile
     if (t_first < t_end && tid < NMOM * TZ) {
         int inst, zt;
@@ -241,13 +263,26 @@ __global__ void __launch_bounds__(tma::NTHR, MINB)
     consumer_sync();
 
     uint32_t it = 0;
+    int4 cur = make_int4(0, 0, 0, 0);
+    if (BATCHED && t_first < t_end) cur = bd.table[t_first];
     for (int t = t_first; t < t_end; t += t_step) {
-        int inst, zt;
-        tma_tile<BATCHED>(bd, t, inst, zt);
+        const int inst = BATCHED ? cur.x : 0, zt = BATCHED ? cur.y : t;
+        const int tn = t + t_step;
+        int4 nxt = cur;
+        if (BATCHED && tn < t_end) nxt = bd.table[tn];  // next tile's entry, one tile ahead
         const StageArgs &a = BATCHED ? bd.args[inst * 4 + STAGE - 1] : a0;
-        const int nch = (a.nvz + R - 1) / R;
-        const bool coll = (a.flags & F_COLL) != 0;
-        const bool advec = (a.flags & F_ADVEC_OFF) == 0;
+        // the member's fields in registers for the whole tile: batched, the
+        // arguments live in global memory and the compiler would reload them
+        // after every store to U / A, which it cannot prove they do not alias
+        TOUT *const U_ = static_cast<TOUT *>(a.U);
+        double *const A_ = a.A;
+        const long long cs_ = a.cs;
+        const int nz_ = a.nz, nvz_ = a.nvz, ld_ = a.ld, H_ = a.H, flags_ = a.flags;
+        const int fda_ = a.fd_advec, kord_ = a.ko_order;
+        const double v0_ = a.v0, dv_ = a.dv, dz_ = a.dz;
+        const int nch = (nvz_ + R - 1) / R;
+        const bool coll = (flags_ & F_COLL) != 0;
+        const bool advec = (flags_ & F_ADVEC_OFF) == 0;
         const bool open_bc = a.bc != 0;
         const double dt = a.dt;
         const TC pmo = (TC)a.pmo, ct = (TC)a.ct, st = (TC)a.st, mudv = (TC)(a.mu * a.dv);
@@ -256,10 +291,8 @@ __global__ void __launch_bounds__(tma::NTHR, MINB)
         const int z = z0 + lane;
         // prefetch the next tile's input moments into a register
         double mnext = 0.0;
-        const int tn = t + t_step;
         if (tid < NMOM * TZ && tn < t_end) {
-            int in2, zn;
-            tma_tile<BATCHED>(bd, tn, in2, zn);
+            const int in2 = BATCHED ? nxt.x : 0, zn = BATCHED ? nxt.y : tn;
             const StageArgs &an = BATCHED ? bd.args[in2 * 4 + STAGE - 1] : a0;
             if (an.flags & F_COLL)
                 mnext = an.Min[(long long)(tid / TZ) * an.nz + zn * TZ + tid % TZ];
@@ -272,10 +305,10 @@ __global__ void __launch_bounds__(tma::NTHR, MINB)
         for (int ch = 0; ch < nch; ++ch, ++it) {
             const int b = it % NBUF;
             const int v = ch * R + warp;
-            const bool valid = v < a.nvz;
-            const int vr = valid ? v : a.nvz - 1;
+            const bool valid = v < nvz_;
+            const int vr = valid ? v : nvz_ - 1;
             double vzv, fac;
-            row_values<SCHEME>(a, vr, vzv, fac);
+            row_values<SCHEME>(v0_, dv_, dz_, fda_, vr, vzv, fac);
             const TC factor = (TC)fac;
             tma::mbar_wait(&full[b], (it / NBUF) & 1, err, 2);
             const unsigned char *buf = smem + b * L::BUF;
@@ -319,13 +352,13 @@ __global__ void __launch_bounds__(tma::NTHR, MINB)
                             // lflux[nz] = 2 lflux[nz-1] - lflux[nz-2]
                             const TC fm1 = __shfl_sync(0xffffffffu, fown, lane > 0 ? lane - 1 : 0);
                             if (dir > 0 && z == 0) fnb = fown;
-                            if (dir < 0 && z == a.nz - 1) fnb = fown * TC(2) - fm1;
+                            if (dir < 0 && z == nz_ - 1) fnb = fown * TC(2) - fm1;
                         }
                         adv = dir > 0 ? factor * (fown - fnb) : factor * (fnb - fown);
                     }
                     o[q] = adv;
                 }
-                if (a.flags & F_VAC) {
+                if (flags_ & F_VAC) {
                     o[EE] += TC(-2) * st * c[EXI] * pmo;
                     o[XX] += TC(2) * st * c[EXI] * pmo;
                     o[EXR] += TC(-2) * ct * c[EXI] * pmo;
@@ -335,7 +368,7 @@ __global__ void __launch_bounds__(tma::NTHR, MINB)
                     o[BEXR] += TC(-2) * ct * c[BEXI] * pmo;
                     o[BEXI] += (TC(2) * ct * c[BEXR] + st * (c[BEE] - c[BXX])) * pmo;
                 }
-                if (a.flags & F_MAT) {
+                if (flags_ & F_MAT) {
                     o[EXR] += hm * c[EXI];
                     o[EXI] += -hm * c[EXR];
                     o[BEXR] += -hm * c[BEXI];
@@ -345,7 +378,7 @@ __global__ void __launch_bounds__(tma::NTHR, MINB)
                 // FD: vacuum, matter, advection, (collective below), dissipation
 #pragma unroll
                 for (int q = 0; q < NCOMP; ++q) o[q] = TC(0);
-                if (a.flags & F_VAC) {
+                if (flags_ & F_VAC) {
                     o[EE] = -pmo * TC(2) * st * c[EXI];
                     o[XX] = pmo * TC(2) * st * c[EXI];
                     o[EXR] = -pmo * TC(2) * ct * c[EXI];
@@ -355,7 +388,7 @@ __global__ void __launch_bounds__(tma::NTHR, MINB)
                     o[BEXR] = -pmo * TC(2) * ct * c[BEXI];
                     o[BEXI] = pmo * (TC(2) * ct * c[BEXR] + st * (c[BEE] - c[BXX]));
                 }
-                if (a.flags & F_MAT) {
+                if (flags_ & F_MAT) {
                     o[EXR] += hm * c[EXI];
                     o[EXI] += -hm * c[EXR];
                     o[BEXR] += -hm * c[BEXI];
@@ -370,9 +403,9 @@ __global__ void __launch_bounds__(tma::NTHR, MINB)
                     const TC m2 = (TC)p[-2], m1 = (TC)p[-1], p1 = (TC)p[1], p2 = (TC)p[2];
                     if (advec) {
                         TC adv;
-                        if (!GEN || a.fd_advec == 0) {
+                        if (!GEN || fda_ == 0) {
                             adv = factor * ((m2 - p2) - TC(8) * (m1 - p1));
-                        } else if (a.fd_advec == 1) {
+                        } else if (fda_ == 1) {
                             adv = factor * (TC(-4) * (TC)p[-3 * sv] + TC(18) * (TC)p[-2 * sv] -
                                             TC(36) * (TC)p[-sv] + TC(22) * c[q]);
                         } else {
@@ -381,7 +414,7 @@ __global__ void __launch_bounds__(tma::NTHR, MINB)
                         }
                         o[q] += adv;
                     }
-                    if (GEN && a.ko_order == 5)
+                    if (GEN && kord_ == 5)
                         ko[q] = ko_eps * ((TC)p[-3] + (TC)p[3] - TC(6) * (m2 + p2) +
                                           TC(15) * (m1 + p1) - TC(20) * c[q]);
                     else
@@ -435,24 +468,24 @@ __global__ void __launch_bounds__(tma::NTHR, MINB)
                     uleft[q] = __shfl_sync(0xffffffffu, u[q], lane > 0 ? lane - 1 : 0);
             }
             if (valid) {
-                TOUT *U = static_cast<TOUT *>(a.U);
-                const long long ro = (long long)v * a.ld + HP;
+                TOUT *U = U_;
+                const long long ro = (long long)v * ld_ + HP;
 #pragma unroll
                 for (int q = 0; q < NCOMP; ++q) {
-                    TOUT *row = U + q * a.cs + ro;
+                    TOUT *row = U + q * cs_ + ro;
                     row[z] = u[q];
-                    if (STAGE <= 3) a.A[q * a.cs + ro + z] = anew[q];
+                    if (STAGE <= 3) A_[q * cs_ + ro + z] = anew[q];
                     if (!open_bc) {
-                        if (z < a.H) row[z + a.nz] = u[q];
-                        if (z >= a.nz - a.H) row[z - a.nz] = u[q];
+                        if (z < H_) row[z + nz_] = u[q];
+                        if (z >= nz_ - H_) row[z - nz_] = u[q];
                     } else {
                         if (z == 0)
-                            for (int g = 1; g <= a.H; ++g) row[-g] = u[q];
-                        if (z == a.nz - 1) {
+                            for (int g = 1; g <= H_; ++g) row[-g] = u[q];
+                        if (z == nz_ - 1) {
                             TOUT p0 = uleft[q], p1 = u[q];
-                            for (int g = 0; g < a.H; ++g) {
+                            for (int g = 0; g < H_; ++g) {
                                 TOUT gh = p1 * TOUT(2) - p0;
-                                row[a.nz + g] = gh;
+                                row[nz_ + g] = gh;
                                 p0 = p1;
                                 p1 = gh;
                             }
@@ -492,11 +525,12 @@ __global__ void __launch_bounds__(tma::NTHR, MINB)
                 double s = 0.0;
 #pragma unroll
                 for (int w = 0; w < R / 2; ++w) s += s_red[w][m][zz];
-                if (coll) a.Mout[(long long)m * a.nz + z0 + zz] = s;
+                if (coll) a.Mout[(long long)m * nz_ + z0 + zz] = s;
                 s_mom[m][zz] = mnext;  // every consumer read this tile's values above
             }
             consumer_sync();
         }
+        cur = nxt;
     }
 }
 

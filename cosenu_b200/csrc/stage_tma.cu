@@ -138,6 +138,8 @@ template <class TIN, int STAGE> struct Layout {
 
 }  // namespace tma
 
+static_assert(sizeof(StageArgs) % 8 == 0, "StageArgs is copied to shared memory in 8-byte words");
+
 template <bool BATCHED>
 __device__ __forceinline__ void tma_tile(const BatchDev &bd, int t, int &inst, int &zt)
 {
@@ -185,6 +187,7 @@ __global__ void __launch_bounds__(tma::NTHR, MINB)
     uint64_t *empty = full + NBUF;
     double(*s_mom)[TZ] = reinterpret_cast<double(*)[TZ]>(empty + NBUF);  // [6][TZ]
     double(*s_red)[NMOM][TZ] = reinterpret_cast<double(*)[NMOM][TZ]>(s_mom + NMOM);  // [R/2]
+    StageArgs *s_args = reinterpret_cast<StageArgs *>(s_red + R / 2);  // batched: current member
 
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const int nzt = BATCHED ? bd.ntiles : a0.nz / TZ;
@@ -263,6 +266,7 @@ __global__ void __launch_bounds__(tma::NTHR, MINB)
     consumer_sync();
 
     uint32_t it = 0;
+    int s_inst = -1;  // member whose arguments s_args holds
     int4 cur = make_int4(0, 0, 0, 0);
     if (BATCHED && t_first < t_end) cur = bd.table[t_first];
     for (int t = t_first; t < t_end; t += t_step) {
@@ -270,23 +274,22 @@ __global__ void __launch_bounds__(tma::NTHR, MINB)
         const int tn = t + t_step;
         int4 nxt = cur;
         if (BATCHED && tn < t_end) nxt = bd.table[tn];  // next tile's entry, one tile ahead
-        const StageArgs &a = BATCHED ? bd.args[inst * 4 + STAGE - 1] : a0;
-        // the member's fields in registers for the whole tile: batched, the
-        // arguments live in global memory and the compiler would reload them
-        // after every store to U / A, which it cannot prove they do not alias
-        TOUT *const U_ = static_cast<TOUT *>(a.U);
-        double *const A_ = a.A;
-        const long long cs_ = a.cs;
-        const int nz_ = a.nz, nvz_ = a.nvz, ld_ = a.ld, H_ = a.H, flags_ = a.flags;
-        const int fda_ = a.fd_advec, kord_ = a.ko_order;
-        const double v0_ = a.v0, dv_ = a.dv, dz_ = a.dz;
-        const int nch = (nvz_ + R - 1) / R;
-        const bool coll = (flags_ & F_COLL) != 0;
-        const bool advec = (flags_ & F_ADVEC_OFF) == 0;
+        if (BATCHED && inst != s_inst) {
+            // a new member: its arguments into shared memory.  Read from there
+            // (like a0 from parameter space) they cost no registers across the
+            // chunk loop and cannot alias the stores to U and A.  The previous
+            // tile's epilogue ended with a consumer barrier.
+            if (tid < (int)(sizeof(StageArgs) / 8))
+                reinterpret_cast<long long *>(s_args)[tid] =
+                    reinterpret_cast<const long long *>(&bd.args[inst * 4 + STAGE - 1])[tid];
+            consumer_sync();
+            s_inst = inst;
+        }
+        const StageArgs &a = BATCHED ? *s_args : a0;
+        const int nch = (a.nvz + R - 1) / R;
+        const bool coll = (a.flags & F_COLL) != 0;
+        const bool advec = (a.flags & F_ADVEC_OFF) == 0;
         const bool open_bc = a.bc != 0;
-        const double dt = a.dt;
-        const TC pmo = (TC)a.pmo, ct = (TC)a.ct, st = (TC)a.st, mudv = (TC)(a.mu * a.dv);
-        const TC ko_eps = (TC)a.ko_eps;
         const int z0 = zt * TZ;
         const int z = z0 + lane;
         // prefetch the next tile's input moments into a register
@@ -300,15 +303,14 @@ __global__ void __launch_bounds__(tma::NTHR, MINB)
         double macc[NMOM] = {0, 0, 0, 0, 0, 0};
         const double M0A = s_mom[0][lane], M0B = s_mom[1][lane], M0C = s_mom[2][lane],
                      M1A = s_mom[3][lane], M1B = s_mom[4][lane], M1C = s_mom[5][lane];
-        const TC hm = (a.flags & F_MAT) ? (TC)a.Hm[z] : TC(0);
 
         for (int ch = 0; ch < nch; ++ch, ++it) {
             const int b = it % NBUF;
             const int v = ch * R + warp;
-            const bool valid = v < nvz_;
-            const int vr = valid ? v : nvz_ - 1;
+            const bool valid = v < a.nvz;
+            const int vr = valid ? v : a.nvz - 1;
             double vzv, fac;
-            row_values<SCHEME>(v0_, dv_, dz_, fda_, vr, vzv, fac);
+            row_values<SCHEME>(a.v0, a.dv, a.dz, a.fd_advec, vr, vzv, fac);
             const TC factor = (TC)fac;
             tma::mbar_wait(&full[b], (it / NBUF) & 1, err, 2);
             const unsigned char *buf = smem + b * L::BUF;
@@ -352,13 +354,16 @@ __global__ void __launch_bounds__(tma::NTHR, MINB)
                             // lflux[nz] = 2 lflux[nz-1] - lflux[nz-2]
                             const TC fm1 = __shfl_sync(0xffffffffu, fown, lane > 0 ? lane - 1 : 0);
                             if (dir > 0 && z == 0) fnb = fown;
-                            if (dir < 0 && z == nz_ - 1) fnb = fown * TC(2) - fm1;
+                            if (dir < 0 && z == a.nz - 1) fnb = fown * TC(2) - fm1;
                         }
                         adv = dir > 0 ? factor * (fown - fnb) : factor * (fnb - fown);
                     }
                     o[q] = adv;
                 }
-                if (flags_ & F_VAC) {
+                if (a.flags & F_VAC) {
+                    // read where used: batched, a is in shared memory and a
+                    // per-tile copy would hold registers across the chunk loop
+                    const TC pmo = (TC)a.pmo, ct = (TC)a.ct, st = (TC)a.st;
                     o[EE] += TC(-2) * st * c[EXI] * pmo;
                     o[XX] += TC(2) * st * c[EXI] * pmo;
                     o[EXR] += TC(-2) * ct * c[EXI] * pmo;
@@ -368,7 +373,8 @@ __global__ void __launch_bounds__(tma::NTHR, MINB)
                     o[BEXR] += TC(-2) * ct * c[BEXI] * pmo;
                     o[BEXI] += (TC(2) * ct * c[BEXR] + st * (c[BEE] - c[BXX])) * pmo;
                 }
-                if (flags_ & F_MAT) {
+                if (a.flags & F_MAT) {
+                    const TC hm = (TC)a.Hm[z];
                     o[EXR] += hm * c[EXI];
                     o[EXI] += -hm * c[EXR];
                     o[BEXR] += -hm * c[BEXI];
@@ -378,7 +384,10 @@ __global__ void __launch_bounds__(tma::NTHR, MINB)
                 // FD: vacuum, matter, advection, (collective below), dissipation
 #pragma unroll
                 for (int q = 0; q < NCOMP; ++q) o[q] = TC(0);
-                if (flags_ & F_VAC) {
+                if (a.flags & F_VAC) {
+                    // read where used: batched, a is in shared memory and a
+                    // per-tile copy would hold registers across the chunk loop
+                    const TC pmo = (TC)a.pmo, ct = (TC)a.ct, st = (TC)a.st;
                     o[EE] = -pmo * TC(2) * st * c[EXI];
                     o[XX] = pmo * TC(2) * st * c[EXI];
                     o[EXR] = -pmo * TC(2) * ct * c[EXI];
@@ -388,13 +397,15 @@ __global__ void __launch_bounds__(tma::NTHR, MINB)
                     o[BEXR] = -pmo * TC(2) * ct * c[BEXI];
                     o[BEXI] = pmo * (TC(2) * ct * c[BEXR] + st * (c[BEE] - c[BXX]));
                 }
-                if (flags_ & F_MAT) {
+                if (a.flags & F_MAT) {
+                    const TC hm = (TC)a.Hm[z];
                     o[EXR] += hm * c[EXI];
                     o[EXI] += -hm * c[EXR];
                     o[BEXR] += -hm * c[BEXI];
                     o[BEXI] += hm * c[BEXR];
                 }
                 const int sv = (vzv > 0.0) - (vzv < 0.0);
+                const TC ko_eps = (TC)a.ko_eps;
                 // one pass over each stencil: advection now, dissipation kept
                 // for after the collective term (the reference's order)
 #pragma unroll
@@ -403,9 +414,9 @@ __global__ void __launch_bounds__(tma::NTHR, MINB)
                     const TC m2 = (TC)p[-2], m1 = (TC)p[-1], p1 = (TC)p[1], p2 = (TC)p[2];
                     if (advec) {
                         TC adv;
-                        if (!GEN || fda_ == 0) {
+                        if (!GEN || a.fd_advec == 0) {
                             adv = factor * ((m2 - p2) - TC(8) * (m1 - p1));
-                        } else if (fda_ == 1) {
+                        } else if (a.fd_advec == 1) {
                             adv = factor * (TC(-4) * (TC)p[-3 * sv] + TC(18) * (TC)p[-2 * sv] -
                                             TC(36) * (TC)p[-sv] + TC(22) * c[q]);
                         } else {
@@ -414,7 +425,7 @@ __global__ void __launch_bounds__(tma::NTHR, MINB)
                         }
                         o[q] += adv;
                     }
-                    if (GEN && kord_ == 5)
+                    if (GEN && a.ko_order == 5)
                         ko[q] = ko_eps * ((TC)p[-3] + (TC)p[3] - TC(6) * (m2 + p2) +
                                           TC(15) * (m1 + p1) - TC(20) * c[q]);
                     else
@@ -422,6 +433,7 @@ __global__ void __launch_bounds__(tma::NTHR, MINB)
                 }
             }
             if (coll) {
+                const TC mudv = (TC)(a.mu * a.dv);
                 const TC SA = (TC)(M0A - vzv * M1A), SB = (TC)(M0B - vzv * M1B),
                          SC = (TC)(M0C - vzv * M1C);
                 const TC Iee = TC(2) * (c[EXR] * SA - c[EXI] * SB);
@@ -441,6 +453,7 @@ __global__ void __launch_bounds__(tma::NTHR, MINB)
             }
 
             // stage combine
+            const double dt = a.dt;
             TOUT u[NCOMP];
             double anew[NCOMP];
 #pragma unroll
@@ -468,24 +481,24 @@ __global__ void __launch_bounds__(tma::NTHR, MINB)
                     uleft[q] = __shfl_sync(0xffffffffu, u[q], lane > 0 ? lane - 1 : 0);
             }
             if (valid) {
-                TOUT *U = U_;
-                const long long ro = (long long)v * ld_ + HP;
+                TOUT *U = static_cast<TOUT *>(a.U);
+                const long long ro = (long long)v * a.ld + HP;
 #pragma unroll
                 for (int q = 0; q < NCOMP; ++q) {
-                    TOUT *row = U + q * cs_ + ro;
+                    TOUT *row = U + q * a.cs + ro;
                     row[z] = u[q];
-                    if (STAGE <= 3) A_[q * cs_ + ro + z] = anew[q];
+                    if (STAGE <= 3) a.A[q * a.cs + ro + z] = anew[q];
                     if (!open_bc) {
-                        if (z < H_) row[z + nz_] = u[q];
-                        if (z >= nz_ - H_) row[z - nz_] = u[q];
+                        if (z < a.H) row[z + a.nz] = u[q];
+                        if (z >= a.nz - a.H) row[z - a.nz] = u[q];
                     } else {
                         if (z == 0)
-                            for (int g = 1; g <= H_; ++g) row[-g] = u[q];
-                        if (z == nz_ - 1) {
+                            for (int g = 1; g <= a.H; ++g) row[-g] = u[q];
+                        if (z == a.nz - 1) {
                             TOUT p0 = uleft[q], p1 = u[q];
-                            for (int g = 0; g < H_; ++g) {
+                            for (int g = 0; g < a.H; ++g) {
                                 TOUT gh = p1 * TOUT(2) - p0;
-                                row[nz_ + g] = gh;
+                                row[a.nz + g] = gh;
                                 p0 = p1;
                                 p1 = gh;
                             }
@@ -525,7 +538,7 @@ __global__ void __launch_bounds__(tma::NTHR, MINB)
                 double s = 0.0;
 #pragma unroll
                 for (int w = 0; w < R / 2; ++w) s += s_red[w][m][zz];
-                if (coll) a.Mout[(long long)m * nz_ + z0 + zz] = s;
+                if (coll) a.Mout[(long long)m * a.nz + z0 + zz] = s;
                 s_mom[m][zz] = mnext;  // every consumer read this tile's values above
             }
             consumer_sync();
@@ -587,7 +600,8 @@ template <class TIN, int STAGE>
 static int tma_smem(int NB)
 {
     using L = tma::Layout<TIN, STAGE>;
-    return NB * L::BUF + 2 * NB * 8 + (1 + tma::R / 2) * NMOM * tma::TZ * 8;
+    return NB * L::BUF + 2 * NB * 8 + (1 + tma::R / 2) * NMOM * tma::TZ * 8 +
+           (int)sizeof(StageArgs);
 }
 
 static int tma_smem_limit(int minb)

@@ -55,7 +55,6 @@ struct BatchDev {
     const StageArgs *args;      // [instances][4]
     const CUtensorMap *maps;    // [instances][5]
     const int *range;           // TMA family: block b owns table entries [range[b], range[b+1])
-    int tab;                    // TMA family: room for per-row tables (max nvz)
 };
 
 // Layout helpers shared by host and device code.

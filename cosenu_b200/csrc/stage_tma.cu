@@ -589,7 +589,8 @@ int make_state_map(CUtensorMap *map, const void *base, int elem_bytes, int ld, i
 
 int tma_box_x() { return tma::XW; }
 int tma_box_tile() { return tma::TZ; }
-// largest nvz the per-row tables in shared memory allow
+// largest nvz the TMA layout is offered for (the range its tests cover; the
+// kernel itself keeps no per-row state in shared memory)
 int tma_max_nvz() { return TMA_MAX_NVZ; }
 
 static const int TMA_SMEM_MAX = 232448;  // opt-in shared memory per block on sm_100

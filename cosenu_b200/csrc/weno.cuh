@@ -10,10 +10,12 @@ namespace cosenu {
 // (rflux of src/rhs_fv.hpp:37-71).  Smoothness indicators and candidate
 // polynomials of the four 4-point sub-stencils; nonlinear weights
 // gamma_r / (eps + beta_r)^2 with gamma = (4, 18, 12, 1)/35 and eps = 1e-6.
-// FP64: the indicators are evaluated on differences from the centre value d
-// (they are invariant under a constant shift: 10 fewer FP64 operations per
-// face and less cancellation), and the four weights are brought to a common
-// denominator so that the face needs one division.
+// FP64: the indicators and the candidate values are evaluated on differences
+// from the centre value d (the indicators are invariant under a constant
+// shift and each candidate's weights sum to 12, so the face is d plus the
+// weighted differences: 15 fewer FP64 operations per face and less
+// cancellation), and the four weights are brought to a common denominator so
+// that the face needs one division.
 __device__ __forceinline__ double weno7_face(double a, double b, double c, double d, double e,
                                              double f, double g)
 {
@@ -27,11 +29,11 @@ __device__ __forceinline__ double weno7_face(double a, double b, double c, doubl
                 547. * E * E;
     double s3 = A * (547. * A - 3882. * B + 4642. * Cc) + B * (7043. * B - 17246. * Cc) +
                 11003. * Cc * Cc;
-    // 12 x candidate values
-    double q0 = 3. * d + 13. * e - 5. * f + g;
-    double q1 = -c + 7. * d + 7. * e - f;
-    double q2 = b - 5. * c + 13. * d + 3. * e;
-    double q3 = -3. * a + 13. * b - 23. * c + 25. * d;
+    // 12 x (candidate value - d): each candidate's weights sum to 12
+    double q0 = 13. * E - 5. * F + G;
+    double q1 = -Cc + 7. * E - F;
+    double q2 = B - 5. * Cc + 3. * E;
+    double q3 = -3. * A + 13. * B - 23. * Cc;
     double d0 = (eps + s0) * (eps + s0);
     double d1 = (eps + s1) * (eps + s1);
     double d2 = (eps + s2) * (eps + s2);
@@ -43,13 +45,12 @@ __device__ __forceinline__ double weno7_face(double a, double b, double c, doubl
     double w3 = d01 * d2;
     double num = w0 * q0 + w1 * q1 + w2 * q2 + w3 * q3;
     double den = 12. * (w0 + w1 + w2 + w3);
-    return num / den;
+    return d + num / den;
 }
 
-// FP32 variant: the indicators are evaluated on differences from the centre
-// value (they are invariant under a constant shift, which removes the
-// cancellation that FP32 would otherwise suffer on O(1) data), and the weights
-// use fast reciprocals.
+// FP32 variant: indicators and candidates on differences from the centre
+// value as above (which removes the cancellation that FP32 would otherwise
+// suffer on O(1) data), and the weights use fast reciprocals.
 __device__ __forceinline__ float weno7_face(float a, float b, float c, float d, float e, float f,
                                             float g)
 {
@@ -63,16 +64,16 @@ __device__ __forceinline__ float weno7_face(float a, float b, float c, float d, 
                547.f * E * E;
     float s3 = A * (547.f * A - 3882.f * B + 4642.f * Cc) + B * (7043.f * B - 17246.f * Cc) +
                11003.f * Cc * Cc;
-    float q0 = 3.f * d + 13.f * e - 5.f * f + g;
-    float q1 = -c + 7.f * d + 7.f * e - f;
-    float q2 = b - 5.f * c + 13.f * d + 3.f * e;
-    float q3 = -3.f * a + 13.f * b - 23.f * c + 25.f * d;
+    float q0 = 13.f * E - 5.f * F + G;
+    float q1 = -Cc + 7.f * E - F;
+    float q2 = B - 5.f * Cc + 3.f * E;
+    float q3 = -3.f * A + 13.f * B - 23.f * Cc;
     float w0 = __fdividef(4.f, (eps + s0) * (eps + s0));
     float w1 = __fdividef(18.f, (eps + s1) * (eps + s1));
     float w2 = __fdividef(12.f, (eps + s2) * (eps + s2));
     float w3 = __fdividef(1.f, (eps + s3) * (eps + s3));
     float num = w0 * q0 + w1 * q1 + w2 * q2 + w3 * q3;
-    return __fdividef(num, 12.f * (w0 + w1 + w2 + w3));
+    return d + __fdividef(num, 12.f * (w0 + w1 + w2 + w3));
 }
 
 }  // namespace cosenu

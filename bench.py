@@ -580,6 +580,69 @@ def run_surrogate(args):
     sur.close()
 
 
+def run_snapshot_study(args):
+    """Cost of writing snapshots while the run continues.  The reference stops
+    the run at every dump and reads the whole state on the host
+    (src/snaps.hpp:187-218).  Three timings of the same K steps on the device
+    timeline: no output; a cosenu_snapshot every N steps (device copy, then the
+    pinned host copy on a side stream, waited for by a host thread as the
+    rho_<t>.dat formatter does); a blocking download every N steps (the
+    reference's pattern)."""
+    import ctypes as C
+    import threading
+
+    import torch
+
+    from cosenu_b200 import NuOsc
+
+    torch.cuda.set_device(0)
+    stream = torch.cuda.Stream()
+    torch.cuda.set_stream(stream)
+    sim = NuOsc(device=0, precision=args.precision, **WORKLOAD)
+    sim.set_stream(stream.cuda_stream)
+    sim.init_seeded(SEED, **IC)
+    sim.evolve(max(args.warmup, 3))
+    torch.cuda.synchronize()
+    K, N = args.steps, args.snapshot_every
+
+    def timed(mode):
+        threads = []
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record(stream)
+        for k in range(0, K, N):
+            sim.evolve(min(N, K - k))
+            if mode == "snapshot":
+                for t in threads:
+                    t.join()  # the host buffer is reused by the next snapshot
+                threads = []
+                sim.snapshot()
+                p = C.POINTER(C.c_double)()
+                t = threading.Thread(target=sim.lib.cosenu_snapshot_wait, args=(sim.h, C.byref(p)))
+                t.start()
+                threads.append(t)
+            elif mode == "download":
+                sim.download()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        for t in threads:
+            t.join()
+        return e0.elapsed_time(e1) / K
+
+    timed("none")  # warm-up
+    ms = {m: timed(m) for m in ("none", "snapshot", "download")}
+    state_bytes = 8 * 8 * WORKLOAD["nz"] * WORKLOAD["nvz"]
+    print(json.dumps({
+        "study": "snapshots while stepping", "workload": WORKLOAD_NAMES[args.workload],
+        "steps": K, "snapshot_every": N, "state_bytes": state_bytes,
+        "ms_per_step": ms,
+        "overhead_per_snapshot_ms": {"snapshot": (ms["snapshot"] - ms["none"]) * N,
+                                     "blocking_download": (ms["download"] - ms["none"]) * N},
+        "precision": args.precision.upper(),
+    }), flush=True)
+    sim.close()
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -596,6 +659,10 @@ def main():
     ap.add_argument("--fp32-study", action="store_true",
                     help="FP32-bulk vs FP64 error study on the chosen workload")
     ap.add_argument("--study-steps", type=int, default=8000)
+    ap.add_argument("--snapshot-study", action="store_true",
+                    help="cost of a snapshot every --snapshot-every steps, asynchronous vs "
+                         "blocking, on the chosen workload")
+    ap.add_argument("--snapshot-every", type=int, default=100)
     ap.add_argument("--t-factor", type=float, default=1000.0, help="c4: run to t_factor/mu")
     ap.add_argument("--workload", choices=sorted(WORKLOADS) + ["c4", "c5"], default="c2",
                     help="c2 (default, the headline): FD 32768 x 256; c1: FV 1024 x 64; "
@@ -620,6 +687,9 @@ def main():
         WORKLOAD.update(nz=args.nz, z0=-0.5 * args.nz * dz, z1=0.5 * args.nz * dz)
     if args.fp32_study:
         run_fp32_study(args)
+        return
+    if args.snapshot_study:
+        run_snapshot_study(args)
         return
     if args.warmup < 3 and args.impl == "ours":
         args.warmup = 3

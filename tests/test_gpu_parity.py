@@ -54,6 +54,20 @@ def test_snapshots_match_reference(gpu_lib, oracle, name, kernel, monkeypatch):
             assert np.all(err <= TOL_PRE), (name, int(t), err)
 
 
+@pytest.mark.parametrize("env", [{"COSENU_TMA_MINB": "1"}, {"COSENU_TMA_RING": "2"},
+                                 {"COSENU_TMA_RING": "4"}])
+def test_tuning_switches_keep_results(gpu_lib, env):
+    """The kernel-shape switches (FV blocks per SM, FD ring depth) change
+    only the schedule: results still match the reference's snapshots."""
+    import subprocess
+    import sys
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    p = subprocess.run([sys.executable, "-m", "tests._env_case", "fv_small", "fd_small",
+                        "fv_open", "fd_open", "fv_mat"], cwd=root, capture_output=True,
+                       text=True, timeout=600, env={**os.environ, **env})
+    assert p.returncode == 0, p.stdout + p.stderr
+
+
 @pytest.mark.parametrize("name", ["fv_small", "fd_small", "fv_vac", "fd_vac", "fv_open",
                                   "fd_ko5", "fv_mat"])
 def test_analysis_matches_reference_tables(gpu_lib, oracle, name):

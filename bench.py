@@ -551,7 +551,7 @@ def run_surrogate(args):
     t0 = time.perf_counter()
     losses = sur.fit(x_train, y_train, epochs=args.epochs, batch=64, lr=2e-3)
     t_fit = time.perf_counter() - t0
-    sur.committee(x_test[:8])  # warm-up
+    sur.committee(x_test)  # warm-up at the timed batch size (activation buffers sized)
     t0 = time.perf_counter()
     mean, spread = sur.committee(x_test)
     t_net = time.perf_counter() - t0
@@ -602,6 +602,8 @@ def run_snapshot_study(args):
     sim.set_stream(stream.cuda_stream)
     sim.init_seeded(SEED, **IC)
     sim.evolve(max(args.warmup, 3))
+    sim.snapshot()  # the first snapshot allocates its device and pinned host buffers
+    sim.snapshot_wait()
     torch.cuda.synchronize()
     K, N = args.steps, args.snapshot_every
 

@@ -60,10 +60,12 @@ WORKLOAD = dict(WORKLOADS["c2"])
 IC = dict(sig_nu=0.6, sig_nubar=0.5, alpha=0.9, amp=1e-6)
 SEED = 20240601
 ANAL_EVERY = 40  # manage.py: N_ITER = 4000 steps, n_analyze = 100
-PASSES = (3, 5, 5, 3)  # state passes (x 64 B) per cell of stages 1..4
-# algorithmic bytes per cell of stages 1..4: FP64 (U in FP64) and FP32-bulk
-# (U in FP32, Y and A in FP64)
-STAGE_BYTES = {"fp64": (192, 320, 320, 192), "fp32": (160, 256, 256, 160)}
+# algorithmic bytes per cell of stages 1..4 (64 B per FP64 state pass).  FP64:
+# stage 1 reads Y, writes U; stage 2 reads U, Y, writes U', A; stage 3 reads
+# U', Y, A, writes U'', A; stage 4 reads U'', A, writes Y (896 B per
+# cell-update).  FP32-bulk (U in FP32, Y and A in FP64): stage 1 also writes A,
+# stage 2 also reads it (832 B).
+STAGE_BYTES = {"fp64": (128, 256, 320, 192), "fp32": (160, 256, 256, 160)}
 FALLBACK_HBM_GBS = 6650.0
 
 
@@ -252,12 +254,12 @@ def run_ours(args):
     result = None
     if rank == 0:
         peak, peak_src = peak_hbm()
-        dom = 1  # stage 2 (5 passes), same kernel shape as stage 3
         sb = STAGE_BYTES[args.precision]
+        dom = max(range(4), key=lambda i: (sb[i], i))  # the stage moving the most bytes
         algo_bytes = sb[dom] * cells
         achieved = algo_bytes / (stage_ms[dom] / 1e3) / 1e9
         tr = traffic_from_profile()
-        key = f"{args.workload}_{args.precision}_stage2_bytes_per_launch"
+        key = f"{args.workload}_{args.precision}_stage{dom + 1}_bytes_per_launch"
         traffic = tr.get(key) if (tr and WORKLOAD["nz"] == WORKLOADS[args.workload]["nz"]) else None
         cpu = cpu_baseline(args) if (world == 1 and not args.no_cpu_baseline) else None
         buf_mb = 8 * WORKLOAD["nvz"] * (WORKLOAD["nz"] + 32) * 8 / 1e6
@@ -282,7 +284,9 @@ def run_ours(args):
             "gpu_launches": 4 * K,
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": traffic,
-                         "kernel": f"rk4_stage_tma_kernel<{sch}, stage 2> (5 state passes)",
+                         "kernel": f"rk4_stage_tma_kernel<{sch}, stage {dom + 1}> "
+                                   f"({sb[dom] // 64 if args.precision == 'fp64' else sb[dom]} "
+                                   f"{'state passes' if args.precision == 'fp64' else 'B/cell'})",
                          "algorithmic_bytes_per_launch": algo_bytes,
                          "avg_launch_ms": stage_ms[dom], "peak_source": peak_src},
             "stage_ms": stage_ms,

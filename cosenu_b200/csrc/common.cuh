@@ -65,4 +65,16 @@ __host__ __device__ inline long long dev_index(long long cs, int ld, int c, int 
 
 inline int padded_ld(int nz) { return ((nz + 2 * HP + 15) / 16) * 16; }
 
+// Three-register RK4 with FP64 stage values: the accumulator A is first
+// written by stage 2 as Y + (U - Y)/3 + dt/3 k2 (U - Y = dt/2 k1 to rounding),
+// so stage 1 writes only U and stage 2 does not read A: 128 fewer bytes per
+// cell-update.  With FP32 stage values U - Y would carry FP32 rounding into
+// the FP64 accumulator, so stage 1 writes A = Y + dt/6 k1 as the reference's
+// vectorize does (src/nuosc.hpp:281-318).
+template <int STAGE, class TIN, class TOUT>
+__host__ __device__ constexpr bool a_from_u()
+{
+    return (STAGE == 1 && sizeof(TOUT) == 8) || (STAGE == 2 && sizeof(TIN) == 8);
+}
+
 }  // namespace cosenu

@@ -280,7 +280,9 @@ __global__ void __launch_bounds__(NTHREADS, 2)
             }
         }
 
-        // stage combine
+        // stage combine (with FP64 stage values, stage 1 leaves A unwritten and
+        // stage 2 forms A = Y + (U - Y)/3 + dt/3 k2, U - Y being dt/2 k1)
+        constexpr bool A_FROM_U = a_from_u<STAGE, TIN, TOUT>();
         TOUT u[NCOMP];
 #pragma unroll
         for (int k = 0; k < NCOMP; ++k) {
@@ -288,11 +290,16 @@ __global__ void __launch_bounds__(NTHREADS, 2)
             const long long idx = k * a.cs + rowoff;
             if (STAGE == 1) {
                 u[k] = (TOUT)(x0[k] + (0.5 * dt) * kk);
-                if (valid) a.A[idx] = x0[k] + (dt / 6.0) * kk;
+                if (!A_FROM_U && valid) a.A[idx] = x0[k] + (dt / 6.0) * kk;
             } else if (STAGE == 2 || STAGE == 3) {
                 const double y = a.Y[idx];
                 u[k] = (TOUT)(y + (STAGE == 2 ? 0.5 * dt : dt) * kk);
-                if (valid) a.A[idx] = a.A[idx] + (dt / 3.0) * kk;
+                if (valid) {
+                    if (A_FROM_U)
+                        a.A[idx] = y + (x0[k] - y) * (1.0 / 3.0) + (dt / 3.0) * kk;
+                    else
+                        a.A[idx] = a.A[idx] + (dt / 3.0) * kk;
+                }
             } else {
                 u[k] = (TOUT)(a.A[idx] + (dt / 6.0) * kk);
             }

@@ -132,7 +132,9 @@ __device__ __forceinline__ void consumer_sync()
 template <class TIN, int STAGE> struct Layout {
     static constexpr int XB = NCOMP * R * XW * (int)sizeof(TIN);
     static constexpr int YB = (STAGE == 2 || STAGE == 3) ? NCOMP * R * TZ * 8 : 0;
-    static constexpr int AB = (STAGE >= 2) ? NCOMP * R * TZ * 8 : 0;
+    // stage 2 reads A only with FP32 stage values (see a_from_u)
+    static constexpr int AB =
+        (STAGE >= 3 || (STAGE == 2 && sizeof(TIN) != 8)) ? NCOMP * R * TZ * 8 : 0;
     static constexpr int BUF = ((XB + YB + AB) + 127) / 128 * 128;
 };
 
@@ -452,7 +454,9 @@ __global__ void __launch_bounds__(tma::NTHR, MINB)
                 for (int q = 0; q < NCOMP; ++q) o[q] += ko[q];
             }
 
-            // stage combine
+            // stage combine (a_from_u: with FP64 stage values stage 1 leaves A
+            // unwritten and stage 2 forms it from U and Y)
+            constexpr bool A_FROM_U = a_from_u<STAGE, TIN, TOUT>();
             const double dt = a.dt;
             TOUT u[NCOMP];
             double anew[NCOMP];
@@ -463,8 +467,12 @@ __global__ void __launch_bounds__(tma::NTHR, MINB)
                     u[q] = (TOUT)(x0[q] + (0.5 * dt) * kk);
                     anew[q] = x0[q] + (dt / 6.0) * kk;
                 } else if (STAGE == 2 || STAGE == 3) {
-                    u[q] = (TOUT)(ys[q * R * TZ] + (STAGE == 2 ? 0.5 * dt : dt) * kk);
-                    anew[q] = as[q * R * TZ] + (dt / 3.0) * kk;
+                    const double y = ys[q * R * TZ];
+                    u[q] = (TOUT)(y + (STAGE == 2 ? 0.5 * dt : dt) * kk);
+                    if (A_FROM_U)
+                        anew[q] = y + (x0[q] - y) * (1.0 / 3.0) + (dt / 3.0) * kk;
+                    else
+                        anew[q] = as[q * R * TZ] + (dt / 3.0) * kk;
                 } else {
                     u[q] = (TOUT)(as[q * R * TZ] + (dt / 6.0) * kk);
                     anew[q] = 0.0;
@@ -487,7 +495,8 @@ __global__ void __launch_bounds__(tma::NTHR, MINB)
                 for (int q = 0; q < NCOMP; ++q) {
                     TOUT *row = U + q * a.cs + ro;
                     row[z] = u[q];
-                    if (STAGE <= 3) a.A[q * a.cs + ro + z] = anew[q];
+                    if (STAGE == 2 || STAGE == 3 || (STAGE == 1 && !A_FROM_U))
+                        a.A[q * a.cs + ro + z] = anew[q];
                     if (!open_bc) {
                         if (z < a.H) row[z + a.nz] = u[q];
                         if (z >= a.nz - a.H) row[z - a.nz] = u[q];

@@ -65,16 +65,27 @@ __host__ __device__ inline long long dev_index(long long cs, int ld, int c, int 
 
 inline int padded_ld(int nz) { return ((nz + 2 * HP + 15) / 16) * 16; }
 
-// Three-register RK4 with FP64 stage values: the accumulator A is first
-// written by stage 2 as Y + (U - Y)/3 + dt/3 k2 (U - Y = dt/2 k1 to rounding),
-// so stage 1 writes only U and stage 2 does not read A: 128 fewer bytes per
-// cell-update.  With FP32 stage values U - Y would carry FP32 rounding into
-// the FP64 accumulator, so stage 1 writes A = Y + dt/6 k1 as the reference's
-// vectorize does (src/nuosc.hpp:281-318).
+// RK4 with FP64 stage values moves 832 B per cell-update instead of 1024:
+// a difference of two stored stage values stands in for each of k1 and k3 in
+// the accumulator (U - Y = dt/2 k1 and U'' - Y = dt k3 to rounding), so
+//   stage 1: U   = Y + dt/2 k1                           (reads Y, writes U)
+//   stage 2: U'  = Y + dt/2 k2, A = Y + (U - Y)/3 + dt/3 k2
+//   stage 3: U'' = Y + dt k3                             (A neither read nor written)
+//   stage 4: Y   = A + (U'' - Y)/3 + dt/6 k4            (reads U'', A, Y)
+// With FP32 stage values a difference would carry FP32 rounding into the FP64
+// accumulator, so A is updated at every stage as the reference's vectorize
+// does (src/nuosc.hpp:281-318).  a_from_u: stage 1 skips A, stage 2 forms it.
 template <int STAGE, class TIN, class TOUT>
 __host__ __device__ constexpr bool a_from_u()
 {
     return (STAGE == 1 && sizeof(TOUT) == 8) || (STAGE == 2 && sizeof(TIN) == 8);
+}
+
+// Stage 3 leaves A alone and stage 4 adds (U'' - Y)/3 (FP64 stage values).
+template <int STAGE, class TIN>
+__host__ __device__ constexpr bool a_lazy34()
+{
+    return (STAGE == 3 || STAGE == 4) && sizeof(TIN) == 8;
 }
 
 }  // namespace cosenu

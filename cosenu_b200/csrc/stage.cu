@@ -280,9 +280,10 @@ __global__ void __launch_bounds__(NTHREADS, 2)
             }
         }
 
-        // stage combine (with FP64 stage values, stage 1 leaves A unwritten and
-        // stage 2 forms A = Y + (U - Y)/3 + dt/3 k2, U - Y being dt/2 k1)
+        // stage combine (FP64 stage values: the accumulator scheme of a_from_u
+        // and a_lazy34 in common.cuh)
         constexpr bool A_FROM_U = a_from_u<STAGE, TIN, TOUT>();
+        constexpr bool A_LAZY = a_lazy34<STAGE, TIN>();
         TOUT u[NCOMP];
 #pragma unroll
         for (int k = 0; k < NCOMP; ++k) {
@@ -297,9 +298,12 @@ __global__ void __launch_bounds__(NTHREADS, 2)
                 if (valid) {
                     if (A_FROM_U)
                         a.A[idx] = y + (x0[k] - y) * (1.0 / 3.0) + (dt / 3.0) * kk;
-                    else
+                    else if (!A_LAZY)
                         a.A[idx] = a.A[idx] + (dt / 3.0) * kk;
                 }
+            } else if (A_LAZY) {
+                const double y = a.Y[idx];  // this thread's own cell, read before its write
+                u[k] = (TOUT)(a.A[idx] + (x0[k] - y) * (1.0 / 3.0) + (dt / 6.0) * kk);
             } else {
                 u[k] = (TOUT)(a.A[idx] + (dt / 6.0) * kk);
             }

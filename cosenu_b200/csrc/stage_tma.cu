@@ -131,10 +131,12 @@ __device__ __forceinline__ void consumer_sync()
 
 template <class TIN, int STAGE> struct Layout {
     static constexpr int XB = NCOMP * R * XW * (int)sizeof(TIN);
-    static constexpr int YB = (STAGE == 2 || STAGE == 3) ? NCOMP * R * TZ * 8 : 0;
-    // stage 2 reads A only with FP32 stage values (see a_from_u)
+    // which of Y and A each stage reads: see a_from_u / a_lazy34 (common.cuh)
+    static constexpr bool FP64U = sizeof(TIN) == 8;
+    static constexpr int YB =
+        (STAGE == 2 || STAGE == 3 || (STAGE == 4 && FP64U)) ? NCOMP * R * TZ * 8 : 0;
     static constexpr int AB =
-        (STAGE >= 3 || (STAGE == 2 && sizeof(TIN) != 8)) ? NCOMP * R * TZ * 8 : 0;
+        (STAGE == 4 || ((STAGE == 2 || STAGE == 3) && !FP64U)) ? NCOMP * R * TZ * 8 : 0;
     static constexpr int BUF = ((XB + YB + AB) + 127) / 128 * 128;
 };
 
@@ -457,6 +459,7 @@ __global__ void __launch_bounds__(tma::NTHR, MINB)
             // stage combine (a_from_u: with FP64 stage values stage 1 leaves A
             // unwritten and stage 2 forms it from U and Y)
             constexpr bool A_FROM_U = a_from_u<STAGE, TIN, TOUT>();
+            constexpr bool A_LAZY = a_lazy34<STAGE, TIN>();
             const double dt = a.dt;
             TOUT u[NCOMP];
             double anew[NCOMP];
@@ -471,8 +474,14 @@ __global__ void __launch_bounds__(tma::NTHR, MINB)
                     u[q] = (TOUT)(y + (STAGE == 2 ? 0.5 * dt : dt) * kk);
                     if (A_FROM_U)
                         anew[q] = y + (x0[q] - y) * (1.0 / 3.0) + (dt / 3.0) * kk;
-                    else
+                    else if (!A_LAZY)
                         anew[q] = as[q * R * TZ] + (dt / 3.0) * kk;
+                    else
+                        anew[q] = 0.0;  // stage 3 leaves A alone
+                } else if (A_LAZY) {
+                    u[q] = (TOUT)(as[q * R * TZ] + (x0[q] - ys[q * R * TZ]) * (1.0 / 3.0) +
+                                  (dt / 6.0) * kk);
+                    anew[q] = 0.0;
                 } else {
                     u[q] = (TOUT)(as[q * R * TZ] + (dt / 6.0) * kk);
                     anew[q] = 0.0;
@@ -495,7 +504,7 @@ __global__ void __launch_bounds__(tma::NTHR, MINB)
                 for (int q = 0; q < NCOMP; ++q) {
                     TOUT *row = U + q * a.cs + ro;
                     row[z] = u[q];
-                    if (STAGE == 2 || STAGE == 3 || (STAGE == 1 && !A_FROM_U))
+                    if (STAGE == 2 || (STAGE == 3 && !A_LAZY) || (STAGE == 1 && !A_FROM_U))
                         a.A[q * a.cs + ro + z] = anew[q];
                     if (!open_bc) {
                         if (z < a.H) row[z + a.nz] = u[q];

@@ -3,12 +3,15 @@
 // One launch = one RK4 stage of NuOsc::step_rk4 (src/nuosc.hpp:320-348):
 // it reads the stage input X with its ghost cells, evaluates the right-hand
 // side of src/rhs_fv.hpp:115-236 (FV, WENO7) or src/rhs_fd.hpp:6-148 (FD),
-// and applies the stage combine of the three-register scheme
+// and applies the stage combine of a three-register RK4 (state Y, stage value
+// U, accumulator A) in the same pass.  With FP32 stage values the accumulator
+// is updated as the reference's vectorize does
 //     stage 1:  U  = Y + dt/2 k1,   A  = Y + dt/6 k1
 //     stage 2:  U' = Y + dt/2 k2,   A += dt/3 k2
 //     stage 3:  U''= Y + dt   k3,   A += dt/3 k3
 //     stage 4:  Y  = A + dt/6 k4
-// in the same pass.  The epilogue also writes the ghost cells of its output
+// and with FP64 stage values differences of stored stage values replace two of
+// those passes (a_from_u / a_lazy34 in common.cuh: 832 B per cell-update).  The epilogue also writes the ghost cells of its output
 // (updateBufferZone, src/nuosc.hpp:212-278, periodic or open) and the six
 // per-z velocity moments of its output that the next stage's collective term
 // needs, so no separate ghost-fill, flux or combine kernels exist.

@@ -61,11 +61,11 @@ IC = dict(sig_nu=0.6, sig_nubar=0.5, alpha=0.9, amp=1e-6)
 SEED = 20240601
 ANAL_EVERY = 40  # manage.py: N_ITER = 4000 steps, n_analyze = 100
 # algorithmic bytes per cell of stages 1..4 (64 B per FP64 state pass).  FP64:
-# stage 1 reads Y, writes U; stage 2 reads U, Y, writes U', A; stage 3 reads
-# U', Y, writes U''; stage 4 reads U'', A, Y, writes Y (832 B per
+# stage 1 reads Y, writes U; stage 2 reads U, Y, writes U'; stage 3 reads U',
+# Y and U, writes U'' and A; stage 4 reads U'', A, writes Y (832 B per
 # cell-update).  FP32-bulk (U in FP32, Y and A in FP64): A updated at every
 # stage as in the reference (160 + 256 + 256 + 160 = 832 B).
-STAGE_BYTES = {"fp64": (128, 256, 192, 256), "fp32": (160, 256, 256, 160)}
+STAGE_BYTES = {"fp64": (128, 192, 320, 192), "fp32": (160, 256, 256, 160)}
 FALLBACK_HBM_GBS = 6650.0
 
 

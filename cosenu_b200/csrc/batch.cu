@@ -277,16 +277,18 @@ int cosenu_batch_create(int n, const cosenu_params *params, cosenu_batch **out)
         b->tv[i] = std::min(params[i].nvz, 64);
     }
     if (cudaMalloc(&b->d_args, 4 * (size_t)n * sizeof(StageArgs)) != cudaSuccess ||
-        cudaMalloc(&b->d_maps, 5 * (size_t)n * sizeof(CUtensorMap)) != cudaSuccess ||
+        cudaMalloc(&b->d_maps, 6 * (size_t)n * sizeof(CUtensorMap)) != cudaSuccess ||
         cudaMalloc(&b->err_flag, 64) != cudaSuccess)
         return bail(COSENU_ERR_NOMEM);
-    std::vector<CUtensorMap> maps(5 * (size_t)n);
+    // per member: Y, U0, U1 input boxes (with halo), Y, A, U0 tile boxes
+    std::vector<CUtensorMap> maps(6 * (size_t)n);
     for (int i = 0; i < n; ++i) {
-        maps[5 * i + 0] = b->m[i]->mY40;
-        maps[5 * i + 1] = b->m[i]->mU0_40;
-        maps[5 * i + 2] = b->m[i]->mU1_40;
-        maps[5 * i + 3] = b->m[i]->mY32;
-        maps[5 * i + 4] = b->m[i]->mA32;
+        maps[6 * i + 0] = b->m[i]->mY40;
+        maps[6 * i + 1] = b->m[i]->mU0_40;
+        maps[6 * i + 2] = b->m[i]->mU1_40;
+        maps[6 * i + 3] = b->m[i]->mY32;
+        maps[6 * i + 4] = b->m[i]->mA32;
+        maps[6 * i + 5] = b->m[i]->mU0_32;
     }
     cudaMemcpyAsync(b->d_maps, maps.data(), maps.size() * sizeof(CUtensorMap),
                     cudaMemcpyHostToDevice, b->stream);

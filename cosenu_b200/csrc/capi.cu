@@ -162,7 +162,9 @@ cudaError_t launch_stage(cosenu_ctx *ctx, int stage, cudaStream_t s)
         const CUtensorMap &mX = stage == 1 ? ctx->mY40 : (stage == 3 ? ctx->mU1_40 : ctx->mU0_40);
         int nblk = std::min(ctx->p.nz / tma_box_tile(),
                             tma_blocks_per_sm(ctx->p.scheme) * ctx->nsm);
-        return launch_rk4_stage_tma(mX, ctx->mY32, ctx->mA32, a, ctx->p.scheme, stage, ctx->fp32,
+        // stage 3 with FP64 stage values reads U at its own cells in the A slot
+        const CUtensorMap &mA = (stage == 3 && !ctx->fp32) ? ctx->mU0_32 : ctx->mA32;
+        return launch_rk4_stage_tma(mX, ctx->mY32, mA, a, ctx->p.scheme, stage, ctx->fp32,
                                     ctx->err_flag, nblk, s);
     }
     return launch_rk4_stage(a, ctx->p.scheme, stage, ctx->tz, ctx->fp32, s);
@@ -420,6 +422,7 @@ int ctx_create(const cosenu_params *pp, cosenu_ctx **out, int layout)
         if (!r) r = make_state_map(&ctx->mU1_40, ctx->U1, ub, ctx->ld, p.nvz, ctx->cs, bx);
         if (!r) r = make_state_map(&ctx->mY32, ctx->Y, 8, ctx->ld, p.nvz, ctx->cs, bt);
         if (!r) r = make_state_map(&ctx->mA32, ctx->A, 8, ctx->ld, p.nvz, ctx->cs, bt);
+        if (!r) r = make_state_map(&ctx->mU0_32, ctx->U0, ub, ctx->ld, p.nvz, ctx->cs, bt);
         if (!r && tma_prepare() != cudaSuccess) r = -2;
         if (r) {
             // no tensor-map support: fall back to the register-tiled kernel

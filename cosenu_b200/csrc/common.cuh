@@ -47,8 +47,8 @@ struct StageArgs {
 
 // Ensemble launch: one stage launch covers every active instance.  Entry t of
 // `table` names (instance, z tile, v tile, rows: nvz in the TMA family); `args` holds the four stage
-// arguments of every instance and `maps` its five tensor maps (Y and U0/U1
-// input boxes, Y and A tile boxes).
+// arguments of every instance and `maps` its six tensor maps (Y and U0/U1
+// input boxes; Y, A and U0 tile boxes).
 struct BatchDev {
     const int4 *table;
     int ntiles;
@@ -66,26 +66,22 @@ __host__ __device__ inline long long dev_index(long long cs, int ld, int c, int 
 inline int padded_ld(int nz) { return ((nz + 2 * HP + 15) / 16) * 16; }
 
 // RK4 with FP64 stage values moves 832 B per cell-update instead of 1024:
-// a difference of two stored stage values stands in for each of k1 and k3 in
-// the accumulator (U - Y = dt/2 k1 and U'' - Y = dt k3 to rounding), so
-//   stage 1: U   = Y + dt/2 k1                           (reads Y, writes U)
-//   stage 2: U'  = Y + dt/2 k2, A = Y + (U - Y)/3 + dt/3 k2
-//   stage 3: U'' = Y + dt k3                             (A neither read nor written)
-//   stage 4: Y   = A + (U'' - Y)/3 + dt/6 k4            (reads U'', A, Y)
+// differences of stored stage values stand in for k1 and k2 in the
+// accumulator (U - Y = dt/2 k1 and U' - Y = dt/2 k2 to rounding), so A is
+// written once, by stage 3, and only stage 3 writes two arrays:
+//   stage 1: U   = Y + dt/2 k1                          (reads Y, writes U)
+//   stage 2: U'  = Y + dt/2 k2                          (reads U, Y, writes U')
+//   stage 3: U'' = Y + dt k3,
+//            A   = Y + (U - Y)/3 + 2 (U' - Y)/3 + dt/3 k3
+//            (reads U', Y and U at its own cells; writes U'' over U, and A)
+//   stage 4: Y   = A + dt/6 k4                          (reads U'', A, writes Y)
 // With FP32 stage values a difference would carry FP32 rounding into the FP64
 // accumulator, so A is updated at every stage as the reference's vectorize
-// does (src/nuosc.hpp:281-318).  a_from_u: stage 1 skips A, stage 2 forms it.
+// does (src/nuosc.hpp:281-318).  a_deferred: this stage uses the FP64 form.
 template <int STAGE, class TIN, class TOUT>
-__host__ __device__ constexpr bool a_from_u()
+__host__ __device__ constexpr bool a_deferred()
 {
-    return (STAGE == 1 && sizeof(TOUT) == 8) || (STAGE == 2 && sizeof(TIN) == 8);
-}
-
-// Stage 3 leaves A alone and stage 4 adds (U'' - Y)/3 (FP64 stage values).
-template <int STAGE, class TIN>
-__host__ __device__ constexpr bool a_lazy34()
-{
-    return (STAGE == 3 || STAGE == 4) && sizeof(TIN) == 8;
+    return (STAGE == 1 && sizeof(TOUT) == 8) || ((STAGE == 2 || STAGE == 3) && sizeof(TIN) == 8);
 }
 
 }  // namespace cosenu

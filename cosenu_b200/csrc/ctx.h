@@ -55,7 +55,7 @@ struct cosenu_ctx {
     // TMA-pipelined FD path: tensor maps over Y, U0, U1 (input boxes) and Y, A
     bool use_tma = false;
     int nsm = 148;
-    CUtensorMap mY40, mU0_40, mU1_40, mY32, mA32;
+    CUtensorMap mY40, mU0_40, mU1_40, mY32, mA32, mU0_32;
     int *err_flag = nullptr;  // device word set by bounded waits that expired
     // graphs of 1 and GRAPH_CHUNK steps
     cudaGraphExec_t g1 = nullptr, gN = nullptr;

@@ -10,8 +10,8 @@
 //     stage 2:  U' = Y + dt/2 k2,   A += dt/3 k2
 //     stage 3:  U''= Y + dt   k3,   A += dt/3 k3
 //     stage 4:  Y  = A + dt/6 k4
-// and with FP64 stage values differences of stored stage values replace two of
-// those passes (a_from_u / a_lazy34 in common.cuh: 832 B per cell-update).  The epilogue also writes the ghost cells of its output
+// and with FP64 stage values stage 3 writes A once from differences of the
+// stored stage values (a_deferred in common.cuh: 832 B per cell-update).  The epilogue also writes the ghost cells of its output
 // (updateBufferZone, src/nuosc.hpp:212-278, periodic or open) and the six
 // per-z velocity moments of its output that the next stage's collective term
 // needs, so no separate ghost-fill, flux or combine kernels exist.
@@ -283,10 +283,9 @@ __global__ void __launch_bounds__(NTHREADS, 2)
             }
         }
 
-        // stage combine (FP64 stage values: the accumulator scheme of a_from_u
-        // and a_lazy34 in common.cuh)
-        constexpr bool A_FROM_U = a_from_u<STAGE, TIN, TOUT>();
-        constexpr bool A_LAZY = a_lazy34<STAGE, TIN>();
+        // stage combine (a_deferred, common.cuh: with FP64 stage values A is
+        // written once, by stage 3)
+        constexpr bool AD = a_deferred<STAGE, TIN, TOUT>();
         TOUT u[NCOMP];
 #pragma unroll
         for (int k = 0; k < NCOMP; ++k) {
@@ -294,19 +293,20 @@ __global__ void __launch_bounds__(NTHREADS, 2)
             const long long idx = k * a.cs + rowoff;
             if (STAGE == 1) {
                 u[k] = (TOUT)(x0[k] + (0.5 * dt) * kk);
-                if (!A_FROM_U && valid) a.A[idx] = x0[k] + (dt / 6.0) * kk;
+                if (!AD && valid) a.A[idx] = x0[k] + (dt / 6.0) * kk;
             } else if (STAGE == 2 || STAGE == 3) {
                 const double y = a.Y[idx];
+                // stage 3 (FP64): U at this thread's own cell, read before U'' replaces it
+                const double u0 = (STAGE == 3 && AD) ? (double)static_cast<const TOUT *>(a.U)[idx]
+                                                     : 0.0;
                 u[k] = (TOUT)(y + (STAGE == 2 ? 0.5 * dt : dt) * kk);
                 if (valid) {
-                    if (A_FROM_U)
-                        a.A[idx] = y + (x0[k] - y) * (1.0 / 3.0) + (dt / 3.0) * kk;
-                    else if (!A_LAZY)
+                    if (!AD)
                         a.A[idx] = a.A[idx] + (dt / 3.0) * kk;
+                    else if (STAGE == 3)
+                        a.A[idx] = y + (u0 - y) * (1.0 / 3.0) + (x0[k] - y) * (2.0 / 3.0) +
+                                   (dt / 3.0) * kk;
                 }
-            } else if (A_LAZY) {
-                const double y = a.Y[idx];  // this thread's own cell, read before its write
-                u[k] = (TOUT)(a.A[idx] + (x0[k] - y) * (1.0 / 3.0) + (dt / 6.0) * kk);
             } else {
                 u[k] = (TOUT)(a.A[idx] + (dt / 6.0) * kk);
             }

@@ -45,6 +45,9 @@ constexpr int R = 8;             // rows per chunk = consumer warps
 constexpr int NCONS = R * 32;    // consumer threads
 constexpr int NTHR = NCONS + 32; // + producer warp
 constexpr unsigned long long WAIT_NS = 2000000000ull;  // 2 s per wait
+// tensor maps per ensemble member: Y, U0, U1 input boxes (with halo), then
+// the Y, A and U0 tile boxes
+constexpr int NMAP = 6;
 #define TMA_MAX_NVZ 1024
 
 __device__ __forceinline__ uint32_t smem_u32(const void *p)
@@ -131,12 +134,12 @@ __device__ __forceinline__ void consumer_sync()
 
 template <class TIN, int STAGE> struct Layout {
     static constexpr int XB = NCOMP * R * XW * (int)sizeof(TIN);
-    // which of Y and A each stage reads: see a_from_u / a_lazy34 (common.cuh)
+    // which of Y and A each stage reads (a_deferred, common.cuh).  Stage 3
+    // with FP64 stage values loads U (its own cells, about to be overwritten
+    // by U'') into the A slot instead of A.
     static constexpr bool FP64U = sizeof(TIN) == 8;
-    static constexpr int YB =
-        (STAGE == 2 || STAGE == 3 || (STAGE == 4 && FP64U)) ? NCOMP * R * TZ * 8 : 0;
-    static constexpr int AB =
-        (STAGE == 4 || ((STAGE == 2 || STAGE == 3) && !FP64U)) ? NCOMP * R * TZ * 8 : 0;
+    static constexpr int YB = (STAGE == 2 || STAGE == 3) ? NCOMP * R * TZ * 8 : 0;
+    static constexpr int AB = (STAGE >= 3 || (STAGE == 2 && !FP64U)) ? NCOMP * R * TZ * 8 : 0;
     static constexpr int BUF = ((XB + YB + AB) + 127) / 128 * 128;
 };
 
@@ -223,18 +226,20 @@ __global__ void __launch_bounds__(tma::NTHR, MINB)
                 int4 nxt = cur;
                 if (BATCHED && has_next) nxt = bd.table[t + t_step];
                 const int inst = BATCHED ? cur.x : 0, zt = BATCHED ? cur.y : t;
+                constexpr int MA = (STAGE == 3 && a_deferred<STAGE, TIN, TOUT>()) ? 5 : 4;
                 const CUtensorMap *px =
-                    BATCHED ? &bd.maps[inst * 5 + (STAGE == 1 ? 0 : (STAGE == 3 ? 2 : 1))] : &mX;
-                const CUtensorMap *py = BATCHED ? &bd.maps[inst * 5 + 3] : &mY;
-                const CUtensorMap *pa = BATCHED ? &bd.maps[inst * 5 + 4] : &mA;
+                    BATCHED ? &bd.maps[inst * NMAP + (STAGE == 1 ? 0 : (STAGE == 3 ? 2 : 1))]
+                            : &mX;
+                const CUtensorMap *py = BATCHED ? &bd.maps[inst * NMAP + 3] : &mY;
+                const CUtensorMap *pa = BATCHED ? &bd.maps[inst * NMAP + MA] : &mA;
                 const int z0 = zt * TZ;
                 const int nch = ((BATCHED ? cur.w : a0.nvz) + R - 1) / R;
                 for (int ch = 0; ch < nch; ++ch, ++it) {
                     if (BATCHED && ch == 0 && has_next && nxt.x != inst) {
-                        const CUtensorMap *m = &bd.maps[nxt.x * 5];
+                        const CUtensorMap *m = &bd.maps[nxt.x * NMAP];
                         tma::prefetch_map(&m[STAGE == 1 ? 0 : (STAGE == 3 ? 2 : 1)]);
                         if (L::YB) tma::prefetch_map(&m[3]);
-                        if (L::AB) tma::prefetch_map(&m[4]);
+                        if (L::AB) tma::prefetch_map(&m[MA]);
                     }
                     const int b = it % NBUF;
                     if (it >= (uint32_t)NBUF)
@@ -456,10 +461,9 @@ __global__ void __launch_bounds__(tma::NTHR, MINB)
                 for (int q = 0; q < NCOMP; ++q) o[q] += ko[q];
             }
 
-            // stage combine (a_from_u: with FP64 stage values stage 1 leaves A
-            // unwritten and stage 2 forms it from U and Y)
-            constexpr bool A_FROM_U = a_from_u<STAGE, TIN, TOUT>();
-            constexpr bool A_LAZY = a_lazy34<STAGE, TIN>();
+            // stage combine (a_deferred, common.cuh: with FP64 stage values A
+            // is written once, by stage 3, from U (in the A slot), U' and Y)
+            constexpr bool AD = a_deferred<STAGE, TIN, TOUT>();
             const double dt = a.dt;
             TOUT u[NCOMP];
             double anew[NCOMP];
@@ -472,16 +476,13 @@ __global__ void __launch_bounds__(tma::NTHR, MINB)
                 } else if (STAGE == 2 || STAGE == 3) {
                     const double y = ys[q * R * TZ];
                     u[q] = (TOUT)(y + (STAGE == 2 ? 0.5 * dt : dt) * kk);
-                    if (A_FROM_U)
-                        anew[q] = y + (x0[q] - y) * (1.0 / 3.0) + (dt / 3.0) * kk;
-                    else if (!A_LAZY)
+                    if (!AD)
                         anew[q] = as[q * R * TZ] + (dt / 3.0) * kk;
+                    else if (STAGE == 3)
+                        anew[q] = y + (as[q * R * TZ] - y) * (1.0 / 3.0) +
+                                  (x0[q] - y) * (2.0 / 3.0) + (dt / 3.0) * kk;
                     else
-                        anew[q] = 0.0;  // stage 3 leaves A alone
-                } else if (A_LAZY) {
-                    u[q] = (TOUT)(as[q * R * TZ] + (x0[q] - ys[q * R * TZ]) * (1.0 / 3.0) +
-                                  (dt / 6.0) * kk);
-                    anew[q] = 0.0;
+                        anew[q] = 0.0;  // stage 2 leaves A alone
                 } else {
                     u[q] = (TOUT)(as[q * R * TZ] + (dt / 6.0) * kk);
                     anew[q] = 0.0;
@@ -504,8 +505,7 @@ __global__ void __launch_bounds__(tma::NTHR, MINB)
                 for (int q = 0; q < NCOMP; ++q) {
                     TOUT *row = U + q * a.cs + ro;
                     row[z] = u[q];
-                    if (STAGE == 2 || (STAGE == 3 && !A_LAZY) || (STAGE == 1 && !A_FROM_U))
-                        a.A[q * a.cs + ro + z] = anew[q];
+                    if (STAGE == 3 || (!AD && STAGE <= 2)) a.A[q * a.cs + ro + z] = anew[q];
                     if (!open_bc) {
                         if (z < a.H) row[z + a.nz] = u[q];
                         if (z >= a.nz - a.H) row[z - a.nz] = u[q];

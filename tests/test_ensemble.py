@@ -10,7 +10,7 @@ import pytest
 from cosenu_b200.ensemble import Instance, ensemble_instances, steps_to
 
 
-def test_configs3_instance_distribution():
+def test_ensemble_instance_distribution():
     xs = ensemble_instances(256)
     nz = np.array([x.nz for x in xs])
     assert len(xs) == 256

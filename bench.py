@@ -13,7 +13,8 @@ metric is cell-updates/s = nz * nvz * steps / time.
          larger than L2, so no flush is needed between steps.
   e2e    through the public API with host buffers: pinned host state ->
          upload -> K steps with on-device analysis every 40 steps (the
-         reference driver's ANAL_EVERY for this run) -> download.
+         reference driver's ANAL_EVERY for this run) and after the last
+         step -> download.
   cpu_baseline / --impl reference: the reference's own CPU build
          (oracle/_ref, compiled from its sources with its --mcore flags)
          on a z-subset of the same grid, all host threads.
@@ -233,7 +234,9 @@ def run_ours(args):
         n = min(ANAL_EVERY, K - done)
         sim.evolve(n)
         done += n
-        if done % ANAL_EVERY == 0:
+        # the reference driver's cadence, plus the end of the run (so the
+        # leg analyses at least once whatever K is)
+        if done % ANAL_EVERY == 0 or done == K:
             sim.analyse()
             n_anal += 1
     from cosenu_b200.nuosc import _ptrs
@@ -279,9 +282,9 @@ def run_ours(args):
                              if buf_mb > 126 else "inputs fit in L2 (small case)",
                        "instances_per_gpu": 1},
             "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": h2d,
-                    "d2h_bytes_per_step": d2h,
-                    "note": f"upload once, {K} steps, analysis every {ANAL_EVERY} steps, "
-                            "download once"},
+                    "d2h_bytes_per_step": d2h, "n_anal": n_anal,
+                    "note": f"upload once, {K} steps, on-device analysis every {ANAL_EVERY} "
+                            f"steps and after the last ({n_anal} in all), download once"},
             "gpu_launches": 4 * K,
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": traffic,

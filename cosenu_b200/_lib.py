@@ -28,6 +28,7 @@ EXPORTS = (
     "cosenu_init_reference", "cosenu_device_state", "cosenu_upload_device",
     "cosenu_download_device", "cosenu_launches_per_step", "cosenu_tile", "cosenu_device_bytes",
     "cosenu_step_noalloc", "cosenu_snapshot", "cosenu_snapshot_wait",
+    "cosenu_set_wait_limit", "cosenu_test_stall_pipeline",
     "cosenu_batch_create", "cosenu_batch_destroy", "cosenu_batch_last_error",
     "cosenu_batch_size", "cosenu_batch_member", "cosenu_batch_init_seeded", "cosenu_batch_run",
     "cosenu_batch_synchronize", "cosenu_batch_autotune", "cosenu_batch_config",
@@ -95,6 +96,8 @@ def load(path: str | None = None) -> C.CDLL:
         "cosenu_step": (i, [vp, i]),
         "cosenu_step_stage": (i, [vp, i]),
         "cosenu_synchronize": (i, [vp]),
+        "cosenu_set_wait_limit": (i, [vp, d]),
+        "cosenu_test_stall_pipeline": (i, [vp, i]),
         "cosenu_time": (i, [vp, C.POINTER(d), C.POINTER(C.c_longlong)]),
         "cosenu_analyse": (i, [vp, C.POINTER(Diag)]),
         "cosenu_pee_v": (i, [vp, vp, vp]),

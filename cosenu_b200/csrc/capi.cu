@@ -146,6 +146,8 @@ StageArgs stage_args(const cosenu_ctx *ctx, int stage)
     a.ko_eps = ctx->p.ko_order == 5 ? -ko / ctx->dz / 64.0 : -ko / ctx->dz / 16.0;
     a.Y = ctx->Y;
     a.A = ctx->A;
+    a.wait_ns = ctx->wait_ns;
+    a.stall = ctx->stall;
     switch (stage) {
     case 1: a.X = ctx->Y; a.U = ctx->U0; a.Min = ctx->M[2]; a.Mout = ctx->M[0]; break;
     case 2: a.X = ctx->U0; a.U = ctx->U1; a.Min = ctx->M[0]; a.Mout = ctx->M[1]; break;
@@ -171,7 +173,9 @@ cudaError_t launch_stage(cosenu_ctx *ctx, int stage, cudaStream_t s)
 }
 
 // Reads the device error word; non-zero means a bounded wait in a stage
-// kernel expired (the results of that launch are not to be trusted).
+// kernel expired (the results of that launch are not to be trusted).  The
+// word stays set, and every later check reports it, until a new state is
+// uploaded or initialised (prepare_state clears it).
 int check_err_flag(cosenu_ctx *ctx)
 {
     if (!ctx->use_tma) return COSENU_OK;
@@ -214,9 +218,11 @@ cudaError_t capture(cosenu_ctx *ctx, int n, cudaGraphExec_t *out)
     return e;
 }
 
-// Refreshes ghosts and input moments of Y after Y changed outside the stages.
+// Refreshes ghosts and input moments of Y after Y changed outside the stages;
+// a new state also clears the error word of an earlier expired wait.
 int prepare_state(cosenu_ctx *ctx)
 {
+    if (ctx->err_flag) CK(cudaMemsetAsync(ctx->err_flag, 0, sizeof(int), ctx->stream));
     CK(launch_ghost_fill(ctx->Y, ctx->cs, ctx->ld, ctx->p.nz, ctx->p.nvz, ctx->H, ctx->p.bc,
                          ctx->stream));
     if (ctx->p.flags & COSENU_COLL)
@@ -509,6 +515,29 @@ int cosenu_set_collective_pars(cosenu_ctx *ctx, double mu)
     DeviceGuard dg(ctx->p.device);
     CK(cudaStreamSynchronize(ctx->stream));
     ctx->p.mu = mu;
+    drop_graphs(ctx);
+    return COSENU_OK;
+}
+
+int cosenu_set_wait_limit(cosenu_ctx *ctx, double seconds)
+{
+    if (!ctx) return COSENU_ERR_ARG;
+    if (!(seconds >= 1e-6 && seconds <= 600.0))
+        return fail(ctx, COSENU_ERR_ARG, "wait limit must be in [1e-6, 600] s");
+    DeviceGuard dg(ctx->p.device);
+    CK(cudaStreamSynchronize(ctx->stream));
+    ctx->wait_ns = (unsigned long long)(seconds * 1e9);
+    drop_graphs(ctx);
+    return COSENU_OK;
+}
+
+int cosenu_test_stall_pipeline(cosenu_ctx *ctx, int on)
+{
+    if (!ctx) return COSENU_ERR_ARG;
+    if (!ctx->use_tma) return fail(ctx, COSENU_ERR_STATE, "the context does not use the TMA kernel");
+    DeviceGuard dg(ctx->p.device);
+    CK(cudaStreamSynchronize(ctx->stream));
+    ctx->stall = on ? 1 : 0;
     drop_graphs(ctx);
     return COSENU_OK;
 }

@@ -38,9 +38,11 @@ struct StageArgs {
     const double *rowfac;// [nvz] advection factor per row (scheme specific)
     const double *Hm;    // [nz] matter potential
     long long cs;        // component stride (elements)
+    unsigned long long wait_ns;  // time limit of each pipeline wait (TMA kernel)
     int nz, nvz, ld, tv, nvt;
     int H;               // ghost cells written per side
     int bc, flags, fd_advec, ko_order;
+    int stall;           // test hook: the TMA producer issues no copies
     double dt, dv, mu, ct, st, pmo, ko_eps;
     double v0, dz;       // velocity grid origin, cell width (rows recompute vz)
 };

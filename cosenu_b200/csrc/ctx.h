@@ -57,6 +57,8 @@ struct cosenu_ctx {
     int nsm = 148;
     CUtensorMap mY40, mU0_40, mU1_40, mY32, mA32, mU0_32;
     int *err_flag = nullptr;  // device word set by bounded waits that expired
+    unsigned long long wait_ns = 2000000000ull;  // limit of each pipeline wait
+    int stall = 0;            // test hook: TMA producers issue no copies
     // graphs of 1 and GRAPH_CHUNK steps
     cudaGraphExec_t g1 = nullptr, gN = nullptr;
     bool use_graphs = true;

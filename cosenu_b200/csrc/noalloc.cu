@@ -14,7 +14,10 @@
 //
 // The first call on a device looks up that array's device address with
 // cudaGetSymbolAddress (the array's name in host code is only a host-side
-// stand-in); make that first call before any stream capture.  All calls share
+// stand-in); make that first call before any stream capture.  The address is
+// kept per device together with the identity of the device's current context,
+// and looked up again when that context changes (after cudaDeviceReset, for
+// instance): the first call in a new context is again a set-up call.  All calls share
 // the one array: calls whose work overlaps on the GPU (different streams, or
 // different host threads on the same device) race on it and must be ordered by
 // the caller.  Each call clears the part of the array it uses, so nothing from
@@ -26,6 +29,8 @@
 #include <cmath>
 #include <mutex>
 #include <string>
+
+#include <cuda.h>
 
 #include "../../include/cosenu_b200.h"
 #include "common.cuh"
@@ -85,6 +90,35 @@ namespace {
 
 std::mutex g_addr_mutex;
 double *g_addr[64] = {nullptr};
+unsigned long long g_addr_ctx[64] = {0};  // context the cached address belongs to
+
+typedef CUresult (*CtxGetCurrentFn)(CUcontext *);
+typedef CUresult (*CtxGetIdFn)(CUcontext, unsigned long long *);
+
+// Unique id of the current context (0 if the driver cannot say: the address
+// is then looked up on every call).
+unsigned long long current_ctx_id()
+{
+    static CtxGetCurrentFn get_cur = nullptr;
+    static CtxGetIdFn get_id = nullptr;
+    static bool tried = false;
+    if (!tried) {
+        tried = true;
+        void *p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            get_cur = (CtxGetCurrentFn)p;
+        if (cudaGetDriverEntryPoint("cuCtxGetId", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            get_id = (CtxGetIdFn)p;
+    }
+    CUcontext c = nullptr;
+    unsigned long long id = 0;
+    if (!get_cur || !get_id || get_cur(&c) != CUDA_SUCCESS || !c || get_id(c, &id) != CUDA_SUCCESS)
+        return 0;
+    return id;
+}
 
 int noalloc_fail(int code, const std::string &msg)
 {
@@ -145,15 +179,17 @@ extern "C" int cosenu_step_noalloc(const cosenu_params *pp, double *const state[
         if (code != COSENU_OK) return noalloc_fail(code, std::string(what) + ": " + cudaGetErrorString(err));
         return COSENU_OK;
     };
-    // set-up, once per device with that device current
+    // set-up, once per device (and again in a new context) with that device current
     double *base;
     {
         std::lock_guard<std::mutex> lk(g_addr_mutex);
-        if (!g_addr[p.device]) {
+        const unsigned long long ctx_id = current_ctx_id();
+        if (!g_addr[p.device] || ctx_id == 0 || ctx_id != g_addr_ctx[p.device]) {
             void *ptr = nullptr;
             e = cudaGetSymbolAddress(&ptr, g_noalloc_scratch);
             if (e != cudaSuccess) return done(COSENU_ERR_CUDA, "cudaGetSymbolAddress", e);
             g_addr[p.device] = static_cast<double *>(ptr);
+            g_addr_ctx[p.device] = ctx_id;
         }
         base = g_addr[p.device];
     }

@@ -24,9 +24,13 @@
 // FD4 + KO3) is a compile-time fast path; the upwind / lopsided / KO5 variants
 // take the generic path.
 //
-// Every wait is bounded in time (globaltimer): on expiry the kernel records a
-// code in *err and carries on along the same control path, so no barrier is
-// left waiting and the host reports the error.
+// Every wait is bounded in time (globaltimer, limit StageArgs::wait_ns): on
+// expiry the kernel records a code in *err and carries on along the same
+// control path, so no barrier is left waiting and the host reports the error.
+// After a failed wait a consumer warp does not release its buffer, so the
+// producer's next wait on that buffer fails too and it stops issuing copies;
+// before it exits it waits (bounded again) for the copies it has in flight, so
+// no block ends while a bulk copy still writes into its shared memory.
 #include <cuda.h>
 
 #include <type_traits>
@@ -44,7 +48,6 @@ constexpr int XW = TZ + 2 * HALO;
 constexpr int R = 8;             // rows per chunk = consumer warps
 constexpr int NCONS = R * 32;    // consumer threads
 constexpr int NTHR = NCONS + 32; // + producer warp
-constexpr unsigned long long WAIT_NS = 2000000000ull;  // 2 s per wait
 // tensor maps per ensemble member: Y, U0, U1 input boxes (with halo), then
 // the Y, A and U0 tile boxes
 constexpr int NMAP = 6;
@@ -79,10 +82,11 @@ __device__ __forceinline__ bool mbar_try(uint64_t *bar, uint32_t parity)
     return ok != 0;
 }
 
-// Bounded wait; returns false (and records `code`) when the time limit passes.
+// Bounded wait; returns false (and records `code`) when `limit_ns` passes.
 // Once any wait in the grid has expired (*err != 0) later waits give up
 // at once, so a broken pipeline ends within one time limit.
-__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity, int *err, int code)
+__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity, int *err, int code,
+                                          unsigned long long limit_ns)
 {
     if (mbar_try(bar, parity)) return true;
     volatile int *verr = err;
@@ -90,9 +94,25 @@ __device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity, int *e
     const unsigned long long t0 = gtimer();
     for (uint32_t n = 1;; ++n) {
         if (mbar_try(bar, parity)) return true;
-        if ((n & 63) == 0 && (*verr != 0 || gtimer() - t0 > WAIT_NS)) {
+        if ((n & 63) == 0 && (*verr != 0 || gtimer() - t0 > limit_ns)) {
             atomicCAS(err, 0, code);
             return false;
+        }
+    }
+}
+
+// Wait for the completion of copies already issued, whatever *err says
+// (bounded by `limit_ns`, code 3 on expiry): the producer's last act.
+__device__ __forceinline__ void mbar_drain(uint64_t *bar, uint32_t parity, int *err,
+                                           unsigned long long limit_ns)
+{
+    if (mbar_try(bar, parity)) return;
+    const unsigned long long t0 = gtimer();
+    for (uint32_t n = 1;; ++n) {
+        if (mbar_try(bar, parity)) return;
+        if ((n & 63) == 0 && gtimer() - t0 > limit_ns) {
+            atomicCAS(err, 0, 3);
+            return;
         }
     }
 }
@@ -210,8 +230,9 @@ __global__ void __launch_bounds__(tma::NTHR, MINB)
 
     if (warp == R) {
         // ------------------------------------------------------------ producer
-        if (lane == 0) {
+        if (lane == 0 && !a0.stall) {
             uint32_t it = 0;
+            bool issuing = true;  // false once a wait has failed: no further copies
             const bool rr = !BATCHED || bd.range == nullptr;  // interleaved tiles
             const int t_first = rr ? blockIdx.x : bd.range[blockIdx.x];
             const int t_end = rr ? nzt : bd.range[blockIdx.x + 1];
@@ -221,7 +242,7 @@ __global__ void __launch_bounds__(tma::NTHR, MINB)
             // prefetched while the previous tile streams
             int4 cur = make_int4(0, 0, 0, 0);
             if (BATCHED && t_first < t_end) cur = bd.table[t_first];
-            for (int t = t_first; t < t_end; t += t_step) {
+            for (int t = t_first; t < t_end && issuing; t += t_step) {
                 const bool has_next = t + t_step < t_end;
                 int4 nxt = cur;
                 if (BATCHED && has_next) nxt = bd.table[t + t_step];
@@ -242,8 +263,11 @@ __global__ void __launch_bounds__(tma::NTHR, MINB)
                         if (L::AB) tma::prefetch_map(&m[MA]);
                     }
                     const int b = it % NBUF;
-                    if (it >= (uint32_t)NBUF)
-                        tma::mbar_wait(&empty[b], ((it / NBUF) - 1) & 1, err, 1);
+                    if (it >= (uint32_t)NBUF &&
+                        !tma::mbar_wait(&empty[b], ((it / NBUF) - 1) & 1, err, 1, a0.wait_ns)) {
+                        issuing = false;  // a consumer gave up: buffer b may still be in use
+                        break;
+                    }
                     unsigned char *buf = smem + b * L::BUF;
                     tma::mbar_expect_tx(&full[b], L::XB + L::YB + L::AB);
                     tma::tma_load_3d(buf, px, HP + z0 - HALO, ch * R, 0, &full[b]);
@@ -253,6 +277,10 @@ __global__ void __launch_bounds__(tma::NTHR, MINB)
                 }
                 cur = nxt;
             }
+            // the last copy issued into each buffer has landed before the block
+            // may exit (in normal operation the consumers have waited for it)
+            for (uint32_t j = it > (uint32_t)NBUF ? it - NBUF : 0; j < it; ++j)
+                tma::mbar_drain(&full[j % NBUF], (j / NBUF) & 1, err, a0.wait_ns);
         }
         return;
     }
@@ -321,7 +349,7 @@ __global__ void __launch_bounds__(tma::NTHR, MINB)
             double vzv, fac;
             row_values<SCHEME>(a.v0, a.dv, a.dz, a.fd_advec, vr, vzv, fac);
             const TC factor = (TC)fac;
-            tma::mbar_wait(&full[b], (it / NBUF) & 1, err, 2);
+            const bool landed = tma::mbar_wait(&full[b], (it / NBUF) & 1, err, 2, a0.wait_ns);
             const unsigned char *buf = smem + b * L::BUF;
             const TIN *xrow = reinterpret_cast<const TIN *>(buf) + warp * XW + HALO;
             const TIN *xs = xrow + lane;
@@ -488,9 +516,10 @@ __global__ void __launch_bounds__(tma::NTHR, MINB)
                     anew[q] = 0.0;
                 }
             }
-            // this warp is done with the buffer
+            // this warp is done with the buffer (after a failed wait it keeps
+            // the buffer: the producer's wait on it fails and it stops issuing)
             __syncwarp();
-            if (lane == 0) tma::mbar_arrive(&empty[b]);
+            if (lane == 0 && landed) tma::mbar_arrive(&empty[b]);
 
             TOUT uleft[NCOMP];
             if (open_bc) {

@@ -187,6 +187,10 @@ class NuOsc:
     def synchronize(self) -> None:
         self._check(self.lib.cosenu_synchronize(self.h))
 
+    def set_wait_limit(self, seconds: float) -> None:
+        """Time limit of each pipeline wait inside the TMA stage kernels."""
+        self._check(self.lib.cosenu_set_wait_limit(self.h, seconds))
+
     @property
     def phy_time(self) -> float:
         t = C.c_double()

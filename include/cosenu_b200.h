@@ -141,8 +141,22 @@ int cosenu_step(cosenu_ctx *ctx, int nsteps);
  * exposed so that a caller can time the stages separately. */
 int cosenu_step_stage(cosenu_ctx *ctx, int stage);
 
-/* Waits for the context's stream. */
+/* Waits for the context's stream.  COSENU_ERR_CUDA when a pipeline wait of a
+ * stage kernel ran out of time (its results are not to be trusted); that
+ * report repeats on every later check until a new state is uploaded or
+ * initialised.  The reference has no such watchdog (its loops cannot stall). */
 int cosenu_synchronize(cosenu_ctx *ctx);
+
+/* Time limit of every wait inside the TMA-pipelined stage kernels (default
+ * 2 s; range [1e-6, 600] s).  No counterpart in the reference. */
+int cosenu_set_wait_limit(cosenu_ctx *ctx, double seconds);
+
+/* Test hook for the watchdog (no counterpart in the reference): with on != 0
+ * the TMA stage kernels issue no copies, so their consumers' waits run out
+ * after the wait limit and the next check returns COSENU_ERR_CUDA.  Nothing
+ * faults or hangs: every wait is bounded and nothing is in flight.
+ * COSENU_ERR_STATE if the context does not use the TMA kernel. */
+int cosenu_test_stall_pipeline(cosenu_ctx *ctx, int on);
 
 /* Simulated time and number of completed RK4 steps (NuOsc::phy_time). */
 int cosenu_time(const cosenu_ctx *ctx, double *phy_time, long long *steps);
@@ -277,9 +291,11 @@ int cosenu_mlp_train(cosenu_mlp *net, int epochs, int batch, float lr, float wei
  * Working memory is one fixed device array inside the library (20.5 MB, held by
  * every GPU that loads the library until exit): grids need
  * nvz * (nz + 32 rounded up to a multiple of 16) <= 69632 and nz <= 16384
- * (the 1024 x 64 grid fits); larger grids return COSENU_ERR_ARG
- * with the limit in cosenu_last_error(NULL).  The first call on a device looks
- * up that array's address; make it before any stream capture.  Calls share the
+ * (the 1024 x 64 grid fits), and p->tile_v <= 64 (0 picks min(nvz, 64));
+ * larger grids or v tiles return COSENU_ERR_ARG with the limit in
+ * cosenu_last_error(NULL).  The first call on a device (and the first after
+ * the device's context was re-created, e.g. by cudaDeviceReset) looks up that
+ * array's address; make it before any stream capture.  Calls share the
  * array, so calls whose GPU work overlaps race; order them.  Work is queued on
  * `stream` (a cudaStream_t, NULL for the default stream) and not waited for. */
 int cosenu_step_noalloc(const cosenu_params *p, double *const state[8], int ld, int nsteps,

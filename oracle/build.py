@@ -24,7 +24,10 @@ import subprocess
 import sys
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-REF_ROOT = os.environ.get("COSENU_REFERENCE_ROOT", "/root/reference")
+# the COSEnu source tree: COSENU_REFERENCE_ROOT, else a "reference" directory
+# beside this repository's checkout
+REF_ROOT = os.environ.get("COSENU_REFERENCE_ROOT") or os.path.join(
+    os.path.dirname(os.path.dirname(HERE)), "reference")
 REF_OUT = os.path.join(HERE, "_ref")
 ORACLE_SO = os.path.join(HERE, "libcosenu_oracle.so")
 
@@ -104,6 +107,10 @@ def build_reference(force: bool = False) -> dict[str, str]:
 
 def build(force: bool = False) -> None:
     build_oracle(force)
+    if not reference_available():
+        print(f"oracle/build.py: no COSEnu tree at {REF_ROOT} (set COSENU_REFERENCE_ROOT); "
+              "reference binaries not rebuilt", file=sys.stderr)
+        return
     build_reference(force)
 
 

@@ -275,9 +275,10 @@ def read_table(path: str) -> np.ndarray:
 
 def run_reference(case: Case, G, bG, state0, n_iter: int, anal_every: int, n_dump_rho: int,
                   workdir: str | None = None, nthreads: int = 0, exe: str | None = None,
-                  timeout: float = 3600) -> dict:
+                  timeout: float = 3600, read_dumps: bool = True) -> dict:
     """Run the reference binary through its --ff path; returns the files it
-    wrote (text) and the parsed loop time (time.txt)."""
+    wrote (text; the rho_<t>.dat snapshots only with ``read_dumps``, they stay
+    in ``workdir`` otherwise) and the parsed loop time (time.txt)."""
     from oracle.build import ref_binary
     exe = exe or ref_binary(case.ref_variant())
     if not os.path.exists(exe):
@@ -296,6 +297,8 @@ def run_reference(case: Case, G, bG, state0, n_iter: int, anal_every: int, n_dum
         raise RuntimeError(f"reference exited {p.returncode}: {p.stdout[-400:]} {p.stderr[-400:]}")
     files = {}
     for fn in os.listdir(wd):
+        if fn.startswith("rho_") and not read_dumps:
+            continue
         if fn.endswith(".dat") or fn == "time.txt":
             files[fn] = open(os.path.join(wd, fn)).read()
     out = {"files": files, "workdir": wd, "stdout": p.stdout,

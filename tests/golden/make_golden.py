@@ -75,6 +75,79 @@ CASES = {
 SUBSET_STRIDE = 16  # z stride of the stored subset for big cases
 TEXT_PIN_CASES = ("fv_small", "fd_small")
 
+# Full-size grids of the large workloads, truncated to a few steps (the reference
+# needs N_ITER >= 10, src/main.cpp:195).  Each stores a column subset of the
+# dumped state (every v row and component at a few z columns: both periodic
+# edges and seeded random columns), per-row checksums of the whole state and the
+# analysis rows.
+#   name -> (Case kwargs, n_iter, anal_every, n_dump_rho, subset columns)
+FULL_CASES = {
+    # FD (central FD4 + KO3) at nz 32768 x nvz 256: dumps at steps 5 and 10
+    "c2_ref": (dict(nz=32768, nvz=256, gz=2, z0=-3000.0, z1=3000.0, scheme="fd", pmo=1.0,
+                    omega=1e-3, theta_deg=1e-6, mu=1.0), 11, 5, 2, 32),
+    # FV (WENO7) at nz 65536 x nvz 512: analysis at steps 3, 6, 9, dump at step 5
+    "c3_ref": (dict(nz=65536, nvz=512, gz=4, scheme="fv", omega=0.0, mu=1.0), 10, 3, 2, 16),
+}
+
+
+def subset_columns(nz: int, ncol: int) -> np.ndarray:
+    """Both periodic edges (4 columns each) plus seeded random interior columns."""
+    rng = np.random.default_rng(nz)
+    edge = np.concatenate([np.arange(4), np.arange(nz - 4, nz)])
+    rest = np.setdiff1d(np.arange(nz), edge)
+    return np.sort(np.concatenate([edge, rng.choice(rest, ncol - 8, replace=False)]))
+
+
+def row_checksums(s: np.ndarray) -> np.ndarray:
+    """Per component and v row: sum, sum of squares and sum of |x| over z."""
+    return np.stack([s.sum(axis=2), (s * s).sum(axis=2), np.abs(s).sum(axis=2)], -1)
+
+
+def read_rho_dat_fast(path: str, case: Case) -> np.ndarray:
+    """rho_<t>.dat of a large grid -> [8][nvz][nz] (pandas' C tokenizer; the
+    text has z blocks of nvz lines of 10 numbers)."""
+    import pandas as pd
+    a = pd.read_csv(path, sep=r"\s+", header=None, dtype=np.float64, engine="c",
+                    skip_blank_lines=True).to_numpy()
+    a = a.reshape(case.nz, case.nvz, 10)
+    return np.ascontiguousarray(np.transpose(a[:, :, 2:], (2, 1, 0)))
+
+
+def make_full_case(name: str, o: Oracle) -> None:
+    import shutil
+    kw, n_iter, anal, ndump, ncol = FULL_CASES[name]
+    case = Case(**kw)
+    G, bG, st0 = o.init_seeded(case, seed=SEED)
+    wd = tempfile.mkdtemp(prefix=f"cosenu_{name}_")
+    try:
+        r = run_reference(case, G, bG, st0, n_iter=n_iter, anal_every=anal, n_dump_rho=ndump,
+                          workdir=wd, nthreads=os.cpu_count() or 1, timeout=6 * 3600,
+                          read_dumps=False)
+        files = r["files"]
+        dumps = sorted(int(f[4:-4]) for f in os.listdir(wd) if f.startswith("rho_"))
+        cols = subset_columns(case.nz, ncol)
+        s0 = interior(case, st0)
+        out = {"case": json.dumps(kw), "seed": SEED, "n_iter": n_iter, "anal_every": anal,
+               "n_dump_rho": ndump, "dump_steps": np.array(dumps, dtype=np.int64),
+               "columns": cols,
+               "survival_probability": read_table_text(files["survival_probability.dat"]),
+               "conserved_quantities": read_table_text(files["conserved_quantities.dat"]),
+               "ref_loop_seconds": r["loop_seconds"], "ref_threads": os.cpu_count() or 1,
+               "state0_sha256": hashlib.sha256(s0.tobytes()).hexdigest()}
+        for t in dumps:
+            s = read_rho_dat_fast(os.path.join(wd, f"rho_{t}.dat"), case)
+            if not np.all(np.isfinite(s)):
+                raise RuntimeError(f"{name}: reference output at step {t} is not finite")
+            out[f"rho_{t}_columns"] = np.ascontiguousarray(s[:, :, cols])
+            out[f"rho_{t}_row_checksums"] = row_checksums(s)
+            out[f"rho_{t}_pee_v"] = s[0].sum(axis=1) / s0[0].sum(axis=1)
+            out[f"rho_{t}_pbee_v"] = s[4].sum(axis=1) / s0[4].sum(axis=1)
+            del s
+    finally:
+        shutil.rmtree(wd, ignore_errors=True)
+    np.savez_compressed(os.path.join(HERE, f"{name}.npz"), **out)
+    print(f"{name}: dumps {dumps}, loop {r['loop_seconds']:.1f}s")
+
 
 def _b(txt: str) -> np.ndarray:
     """Text stored as raw bytes (uint8) inside the npz."""
@@ -160,10 +233,12 @@ def read_table_text(txt: str) -> np.ndarray:
 def main(argv: list[str]) -> None:
     build()
     o = Oracle()
-    names = argv or list(CASES) + ["fv_default_ic"]
+    names = argv or list(CASES) + ["fv_default_ic"] + list(FULL_CASES)
     for n in names:
         if n == "fv_default_ic":
             make_default_ic(o)
+        elif n in FULL_CASES:
+            make_full_case(n, o)
         else:
             make_case(n, o)
 

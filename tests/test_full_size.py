@@ -1,0 +1,100 @@
+"""The CUDA path at the full sizes of the large workloads, against the
+reference's own runs (tests/golden/c2_ref.npz, c3_ref.npz: the reference
+binary on the full grids, truncated to a few steps).
+
+Compared: every v row and component at a column subset of the dumped state
+(both periodic edges and seeded interior columns) to <= 1e-10 max-abs; per-row
+sums, sums of squares and sums of |x| of the whole state to 1e-11 relative;
+P_ee(v); and the rows of conserved_quantities.dat and
+survival_probability.dat at the reference's analysis steps.
+"""
+import numpy as np
+import pytest
+
+from tests._util import gpu_from_case, load_golden, maxabs_per_comp
+
+pytestmark = pytest.mark.gpu
+
+TOL_PRE = 1e-10
+TOL_CK = 1e-11  # relative, per-row checksums over the whole z extent
+
+
+def _row_checksums(s):
+    return np.stack([s.sum(axis=2), (s * s).sum(axis=2), np.abs(s).sum(axis=2)], -1)
+
+
+def _check_dump(case, d, t, got):
+    cols = d["columns"]
+    err = maxabs_per_comp(got[:, :, cols], d[f"rho_{t}_columns"])
+    assert np.all(err <= TOL_PRE), (t, err)
+    ck, want = _row_checksums(got), d[f"rho_{t}_row_checksums"]
+    rel = np.abs(ck - want) / np.maximum(np.abs(want), 1e-300)
+    # sums of components that are zero to rounding compare in absolute terms
+    ok = (rel <= TOL_CK) | (np.abs(ck - want) <= 1e-13 * case.nz)
+    assert ok.all(), (t, rel.max())
+
+
+def _check_rows(d, t, a):
+    cq = {int(r[0]): r for r in d["conserved_quantities"]}
+    sp = {int(r[0]): r for r in d["survival_probability"]}
+    if t in cq:
+        row = cq[t]
+        got = np.array([a["dP_max"], a["avdP"], a["avbdP"], a["M0"]])
+        assert np.all(np.abs(got - row[1:]) <= 1e-12 * np.maximum(np.abs(row[1:]), 1.0)), \
+            (t, got, row)
+    if t in sp:
+        # survival_probability.dat holds 7 significant digits
+        assert abs(a["Pee"] - sp[t][1]) <= 5e-7 and abs(a["Pbee"] - sp[t][2]) <= 5e-7
+
+
+def _run(name, precision="fp64"):
+    case, d = load_golden(name)
+    steps = sorted(set(int(t) for t in d["dump_steps"]) |
+                   set(int(r[0]) for r in d["conserved_quantities"]))
+    out = {}
+    with gpu_from_case(case, precision=precision) as sim:
+        sim.init_seeded(int(d["seed"]))
+        a0 = sim.analyse()
+        t_prev = 0
+        for t in steps:
+            sim.evolve(t - t_prev)
+            t_prev = t
+            a = sim.analyse()
+            got = None
+            if t in d["dump_steps"]:
+                got = sim.download()[:, :, case.gz:case.gz + case.nz]
+                pee, pbee = sim.pee_v()
+                got = (got, pee, pbee)
+            out[t] = (a, got)
+    return case, d, a0, out
+
+
+def test_fd_benchmark_grid_against_reference_run(gpu_lib):
+    """FD (central FD4 + KO3) at nz 32768 x nvz 256, mu 1, omega 1e-3,
+    theta 1e-6 deg: the reference's dumps at steps 5 and 10 and its analysis
+    rows; trace, anti-trace and ELN conserved to 1e-12 relative."""
+    case, d, a0, out = _run("c2_ref")
+    for t, (a, got) in out.items():
+        _check_rows(d, t, a)
+        if got is not None:
+            s, pee, pbee = got
+            _check_dump(case, d, t, s)
+            assert np.abs(pee - d[f"rho_{t}_pee_v"]).max() <= 1e-12
+            assert np.abs(pbee - d[f"rho_{t}_pbee_v"]).max() <= 1e-12
+        for k in ("trace", "btrace", "eln"):
+            assert abs(a[k] - a0[k]) <= 1e-12 * abs(a0[k]), (t, k, a[k], a0[k])
+
+
+def test_fv_large_grid_against_reference_run(gpu_lib):
+    """FV (WENO7) at nz 65536 x nvz 512, mu 1, omega 0: the reference's dump at
+    step 5 and its analysis rows at steps 3, 6 and 9; trace and ELN conserved."""
+    case, d, a0, out = _run("c3_ref")
+    for t, (a, got) in out.items():
+        _check_rows(d, t, a)
+        if got is not None:
+            s, pee, pbee = got
+            _check_dump(case, d, t, s)
+            assert np.abs(pee - d[f"rho_{t}_pee_v"]).max() <= 1e-12
+            assert np.abs(pbee - d[f"rho_{t}_pbee_v"]).max() <= 1e-12
+        for k in ("trace", "btrace", "eln"):
+            assert abs(a[k] - a0[k]) <= 1e-12 * abs(a0[k]), (t, k, a[k], a0[k])

@@ -225,7 +225,8 @@ def test_c1_after_saturation_1500_steps(gpu_lib, oracle):
 
 def test_c2_full_size_one_step_and_conservation(gpu_lib, oracle):
     """The large FD grid (32768 x 256): one step at full size against the
-    oracle, then trace conservation over further steps."""
+    oracle, then trace, anti-trace and ELN conservation over further steps
+    (omega sin 2 theta ~ 3e-11 leaves ELN conserved far below the bound)."""
     from oracle.oracle import Case
     case = Case(nz=32768, nvz=256, gz=2, z0=-3000.0, z1=3000.0, scheme="fd", pmo=1.0,
                 omega=1e-3, theta_deg=1e-6, mu=1.0)
@@ -242,6 +243,7 @@ def test_c2_full_size_one_step_and_conservation(gpu_lib, oracle):
         a1 = sim.analyse()
     assert abs(a1["trace"] - a0["trace"]) <= 1e-12 * abs(a0["trace"])
     assert abs(a1["btrace"] - a0["btrace"]) <= 1e-12 * abs(a0["btrace"])
+    assert abs(a1["eln"] - a0["eln"]) <= 1e-12 * abs(a0["eln"])
 
 
 def test_errors_are_reported_not_fatal(gpu_lib, oracle):

@@ -23,39 +23,55 @@ from cosenu_b200 import _lib as L
 TOL = 1e-12
 
 
-def _call(p, dev, nz, nsteps):
+def _call(p, dev, ld, nsteps):
     lib = L.load()
     ptrs = L.DPTR8(*[dev[c].data_ptr() for c in range(8)])
-    rc = lib.cosenu_step_noalloc(C.byref(p), ptrs, nz, nsteps, None)
+    rc = lib.cosenu_step_noalloc(C.byref(p), ptrs, ld, nsteps, None)
     assert rc == L.OK, lib.cosenu_last_error(None).decode()
 
 
+FD_SMALL = dict(scheme="fd", nz=512, nvz=48, gz=2, omega=1e-3, theta_deg=1e-6, z0=-256.0,
+                z1=256.0)
+T32x16 = dict(tile_z=32, tile_v=16)
+
+
 @pytest.mark.gpu
-@pytest.mark.parametrize("kw", [
-    dict(scheme="fv", nz=1024, nvz=64, gz=4, omega=0.0),                # the small FV grid
-    dict(scheme="fd", nz=512, nvz=48, gz=2, omega=1e-3, theta_deg=1e-6, z0=-256.0, z1=256.0),
-    dict(scheme="fv", nz=256, nvz=20, gz=4, bc="open", omega=1e-2, theta_deg=37.0, z0=-128.0,
-         z1=128.0),
+@pytest.mark.parametrize("kw,tiles,pad", [
+    (dict(scheme="fv", nz=1024, nvz=64, gz=4, omega=0.0), T32x16, 0),  # the small FV grid
+    (FD_SMALL, T32x16, 0),
+    (dict(scheme="fv", nz=256, nvz=20, gz=4, bc="open", omega=1e-2, theta_deg=37.0, z0=-128.0,
+          z1=128.0), T32x16, 0),
+    # the default v tile (min(nvz, 64)) and a collective-term-free run
+    (dict(FD_SMALL, nvz=96), {}, 0),
+    (dict(FD_SMALL, coll=False), T32x16, 0),
+    # the upwind FD stencil (its row factors come from the scratch tables)
+    (dict(FD_SMALL, fd_advec="upwind", ko_order=5, gz=3), dict(tile_z=16, tile_v=5), 0),
+    # rows of the caller's tensor padded past nz (row pitch ld = nz + 8)
+    (dict(scheme="fv", nz=256, nvz=20, gz=4, omega=1e-2, theta_deg=37.0, z0=-128.0, z1=128.0),
+     T32x16, 8),
 ])
-def test_step_noalloc_matches_context_path(kw):
+def test_step_noalloc_matches_context_path(kw, tiles, pad):
     import torch
-    tiles = dict(tile_z=32, tile_v=16)
     nz, gz = kw["nz"], kw["gz"]
+    ld = nz + pad
     ref = NuOsc(**kw, **tiles)
     ref.init_seeded(7)
     st0 = ref.download()
-    # caller-owned device state: [8][nvz][nz], row pitch nz
-    dev = torch.tensor(np.ascontiguousarray(st0[:, :, gz:gz + nz]), device="cuda")
+    # caller-owned device state: [8][nvz][ld], interior at [..., :nz]
+    host = np.zeros((8, kw["nvz"], ld))
+    host[:, :, :nz] = st0[:, :, gz:gz + nz]
+    dev = torch.tensor(host, device="cuda")
     p = make_params(**kw, **tiles)
     for call in range(2):
-        _call(p, dev, nz, 9)
+        _call(p, dev, ld, 9)
         torch.cuda.synchronize()
         ref.evolve(9)
         want = ref.download()[:, :, gz:gz + nz]
         got = dev.cpu().numpy()
-        err = np.abs(got - want).max()
+        err = np.abs(got[:, :, :nz] - want).max()
         assert err <= TOL, (call, err)
         assert np.isfinite(got).all()
+        assert not got[:, :, nz:].any()  # the row padding is left alone
     ref.close()
 
 

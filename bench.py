@@ -64,9 +64,10 @@ ANAL_EVERY = 40  # manage.py: N_ITER = 4000 steps, n_analyze = 100
 # algorithmic bytes per cell of stages 1..4 (64 B per FP64 state pass).  FP64:
 # stage 1 reads Y, writes U; stage 2 reads U, Y, writes U'; stage 3 reads U',
 # Y and U, writes U'' and A; stage 4 reads U'', A, writes Y (832 B per
-# cell-update).  FP32-bulk (U in FP32, Y and A in FP64): A updated at every
-# stage as in the reference (160 + 256 + 256 + 160 = 832 B).
-STAGE_BYTES = {"fp64": (128, 192, 320, 192), "fp32": (160, 256, 256, 160)}
+# cell-update).  FP32-bulk (FP64 Y, FP32 increments D, 32 B per pass): stage 1
+# reads Y, writes D1; stage 2 reads Y, D1, writes D2; stage 3 reads Y, D2,
+# writes D3; stage 4 reads Y, D3, D1, D2, writes the new Y (576 B).
+STAGE_BYTES = {"fp64": (128, 192, 320, 192), "fp32": (96, 128, 128, 224)}
 FALLBACK_HBM_GBS = 6650.0
 
 

@@ -13,6 +13,11 @@
 // phase advances the members that are still active by the smallest remaining
 // count, with the per-step launches captured once into a CUDA graph and
 // replayed; finished members drop out of the table between phases.
+//
+// FP32-bulk members write each step's new state into their other FP64 buffer
+// (common.cuh), so stage arguments and tensor maps exist per buffer parity.
+// A run starts every member from parity 0; active members then advance
+// together and keep a common parity, so each launch picks one set.
 #include <algorithm>
 #include <cstring>
 #include <map>
@@ -34,7 +39,8 @@ struct cosenu_batch {
     std::vector<cosenu_ctx *> m;
     cudaStream_t stream = nullptr, own_stream = nullptr;
     int nsm = 148;
-    // device arrays: per-member stage args and tensor maps, two tile tables
+    // device arrays: per-parity, per-member stage args [2][n][4] and tensor
+    // maps [2][n][NMAP_B]; two tile tables
     StageArgs *d_args = nullptr;
     CUtensorMap *d_maps = nullptr;
     int4 *d_table[2] = {nullptr, nullptr};
@@ -54,6 +60,8 @@ struct cosenu_batch {
 
 namespace {
 
+constexpr int NMAP_B = 7;  // tensor maps per member (the TMA kernel's NMAP)
+
 int bfail(cosenu_batch *b, int code, const std::string &msg)
 {
     if (b) b->err = msg;
@@ -67,12 +75,16 @@ int bfail(cosenu_batch *b, int code, const std::string &msg)
                                                                     cudaGetErrorString(e_));   \
     } while (0)
 
-// Per-member stage arguments for the current kernel choice, to the device.
+// Per-member stage arguments for the current kernel choice, to the device
+// (both buffer parities).
 int upload_args(cosenu_batch *b)
 {
-    std::vector<StageArgs> args(4 * (size_t)b->n);
-    for (int i = 0; i < b->n; ++i)
-        for (int s = 1; s <= 4; ++s) args[4 * i + s - 1] = ctx_stage_args(b->m[i], s);
+    std::vector<StageArgs> args(8 * (size_t)b->n);
+    for (int par = 0; par < 2; ++par)
+        for (int i = 0; i < b->n; ++i)
+            for (int s = 1; s <= 4; ++s)
+                args[4 * ((size_t)par * b->n + i) + s - 1] =
+                    ctx_stage_args(b->m[i], s, b->fp32 ? par : 0);
     BCK(cudaMemcpyAsync(b->d_args, args.data(), args.size() * sizeof(StageArgs),
                         cudaMemcpyHostToDevice, b->stream));
     BCK(cudaStreamSynchronize(b->stream));
@@ -168,13 +180,18 @@ int run_phase(cosenu_batch *b, const std::vector<int> &active, long long nsteps)
     BCK(cudaMemcpyAsync(b->d_table[k], b->h_table[k], (nt + nrange_int4) * sizeof(int4),
                         cudaMemcpyHostToDevice, b->stream));
     BCK(cudaEventRecord(b->table_ev[k], b->stream));
-    BatchDev bd{b->d_table[k], (int)nt, b->d_args, b->d_maps,
-                reinterpret_cast<const int *>(b->d_table[k] + nt)};
-    if (getenv("COSENU_BATCH_RR")) bd.range = nullptr;
+    BatchDev bd0{b->d_table[k], (int)nt, b->d_args, b->d_maps,
+                 reinterpret_cast<const int *>(b->d_table[k] + nt)};
+    if (getenv("COSENU_BATCH_RR")) bd0.range = nullptr;
     int max_nvz = 0;
     for (int i : active) max_nvz = std::max(max_nvz, b->m[i]->p.nvz);
     const StageArgs a0 = ctx_stage_args(b->m[active[0]], 1);
-    auto launch_step = [&](cudaStream_t s) -> cudaError_t {
+    // the active members' common buffer parity (0 for FP64)
+    int par = b->m[active[0]]->ypar;
+    auto launch_step = [&](cudaStream_t s, int p) -> cudaError_t {
+        BatchDev bd = bd0;
+        bd.args += (size_t)p * 4 * b->n;
+        bd.maps += (size_t)p * NMAP_B * b->n;
         for (int st = 1; st <= 4; ++st) {
             cudaError_t e;
             if (b->use_tma)
@@ -186,8 +203,10 @@ int run_phase(cosenu_batch *b, const std::vector<int> &active, long long nsteps)
         }
         return cudaSuccess;
     };
-    // one graph of up to 16 steps for this phase, replayed
-    const int chunk = (int)std::min<long long>(16, nsteps);
+    // one graph of up to 16 steps for this phase, replayed (FP32-bulk: an even
+    // number of steps, so that every replay starts from the same parity)
+    int chunk = (int)std::min<long long>(16, nsteps);
+    if (b->fp32 && chunk > 1) chunk &= ~1;
     cudaGraphExec_t ge = nullptr;
     {
         cudaStream_t cs;
@@ -196,7 +215,7 @@ int run_phase(cosenu_batch *b, const std::vector<int> &active, long long nsteps)
         cudaError_t e = cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal);
         if (e == cudaSuccess) {
             cudaError_t le = cudaSuccess;
-            for (int i = 0; i < chunk && le == cudaSuccess; ++i) le = launch_step(cs);
+            for (int i = 0; i < chunk && le == cudaSuccess; ++i) le = launch_step(cs, par ^ (i & 1));
             e = cudaStreamEndCapture(cs, &g);
             if (le != cudaSuccess) e = le;
         }
@@ -210,11 +229,18 @@ int run_phase(cosenu_batch *b, const std::vector<int> &active, long long nsteps)
     while (left >= chunk && e == cudaSuccess) {
         e = cudaGraphLaunch(ge, b->stream);
         left -= chunk;
+        if (chunk & 1) par ^= b->fp32;  // (an odd chunk is a single replay)
     }
-    while (left-- > 0 && e == cudaSuccess) e = launch_step(b->stream);
+    while (left-- > 0 && e == cudaSuccess) {
+        e = launch_step(b->stream, par);
+        par ^= b->fp32;
+    }
     b->graphs.push_back(ge);  // released once the stream has drained
     if (e != cudaSuccess) return bfail(b, COSENU_ERR_CUDA, std::string("launch: ") + cudaGetErrorString(e));
-    for (int i : active) b->m[i]->steps += nsteps;
+    for (int i : active) {
+        b->m[i]->steps += nsteps;
+        if (nsteps & 1) ctx_flip(b->m[i]);
+    }
     return COSENU_OK;
 }
 
@@ -276,20 +302,26 @@ int cosenu_batch_create(int n, const cosenu_params *params, cosenu_batch **out)
         b->max_nvz = std::max(b->max_nvz, params[i].nvz);
         b->tv[i] = std::min(params[i].nvz, 64);
     }
-    if (cudaMalloc(&b->d_args, 4 * (size_t)n * sizeof(StageArgs)) != cudaSuccess ||
-        cudaMalloc(&b->d_maps, 6 * (size_t)n * sizeof(CUtensorMap)) != cudaSuccess ||
+    if (cudaMalloc(&b->d_args, 8 * (size_t)n * sizeof(StageArgs)) != cudaSuccess ||
+        cudaMalloc(&b->d_maps, 2 * NMAP_B * (size_t)n * sizeof(CUtensorMap)) != cudaSuccess ||
         cudaMalloc(&b->err_flag, 64) != cudaSuccess)
         return bail(COSENU_ERR_NOMEM);
-    // per member: Y, U0, U1 input boxes (with halo), Y, A, U0 tile boxes
-    std::vector<CUtensorMap> maps(6 * (size_t)n);
-    for (int i = 0; i < n; ++i) {
-        maps[6 * i + 0] = b->m[i]->mY40;
-        maps[6 * i + 1] = b->m[i]->mU0_40;
-        maps[6 * i + 2] = b->m[i]->mU1_40;
-        maps[6 * i + 3] = b->m[i]->mY32;
-        maps[6 * i + 4] = b->m[i]->mA32;
-        maps[6 * i + 5] = b->m[i]->mU0_32;
-    }
+    // per parity and member, in the order of the TMA kernel's MapIdx.  FP64:
+    // Y, U0, U1 input boxes (with halo), Y, A, U0 tiles.  FP32-bulk: the
+    // current Y, D1, D2 input boxes, the D2 tile, -, the D1 tile, the D3 box.
+    std::vector<CUtensorMap> maps(2 * NMAP_B * (size_t)n);
+    for (int par = 0; par < 2; ++par)
+        for (int i = 0; i < n; ++i) {
+            const cosenu_ctx *c = b->m[i];
+            CUtensorMap *mp = &maps[NMAP_B * ((size_t)par * n + i)];
+            mp[0] = c->mYb40[b->fp32 ? par : 0];
+            mp[1] = c->mU0_40;
+            mp[2] = c->mU1_40;
+            mp[3] = b->fp32 ? c->mU1_32 : c->mY32;
+            mp[4] = c->mA32;
+            mp[5] = c->mU0_32;
+            mp[6] = c->mU2_40;
+        }
     cudaMemcpyAsync(b->d_maps, maps.data(), maps.size() * sizeof(CUtensorMap),
                     cudaMemcpyHostToDevice, b->stream);
     cudaMemsetAsync(b->err_flag, 0, 64, b->stream);
@@ -367,6 +399,10 @@ int cosenu_batch_run(cosenu_batch *b, const long long *nsteps)
             rc = bfail(b, COSENU_ERR_ARG, "member " + std::to_string(i) + ": negative steps or no state");
             break;
         }
+    // every member starts from buffer parity 0 (FP32-bulk)
+    for (int i = 0; i < b->n && rc == COSENU_OK; ++i)
+        if (ctx_normalise_parity(b->m[i]) != COSENU_OK)
+            rc = bfail(b, COSENU_ERR_CUDA, cosenu_last_error(b->m[i]));
     while (rc == COSENU_OK) {
         std::vector<int> active;
         long long d = 0;
@@ -422,6 +458,8 @@ int cosenu_batch_autotune(cosenu_batch *b, int trial_steps, char *report, size_t
     std::ostringstream rep;
     auto trial = [&](void) -> float {
         if (apply_tiling(b) != COSENU_OK) return 1e30f;
+        for (int i = 0; i < b->n; ++i)
+            if (ctx_normalise_parity(b->m[i]) != COSENU_OK) return 1e30f;
         if (run_phase(b, all, 1) != COSENU_OK) return 1e30f;  // warm-up (graph capture)
         cudaEventRecord(e0, b->stream);
         if (run_phase(b, all, trial_steps) != COSENU_OK) return 1e30f;

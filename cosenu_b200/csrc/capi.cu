@@ -31,7 +31,8 @@ using namespace cosenu;
 // message for cosenu_last_error(NULL): failures that have no context
 thread_local std::string g_create_error;
 
-static const int GRAPH_CHUNK = 16;
+static const int GRAPH_CHUNK = 16;  // even
+static_assert(GRAPH_CHUNK % 2 == 0, "a chunk leaves the buffer parity unchanged");
 
 #define CK(call)                                                                              \
     do {                                                                                      \
@@ -117,8 +118,9 @@ void choose_tile(cosenu_ctx *ctx, int layout = 0)
     ctx->nvt = (p.nvz + tv - 1) / tv;
 }
 
-StageArgs stage_args(const cosenu_ctx *ctx, int stage)
+StageArgs stage_args(const cosenu_ctx *ctx, int stage, int par)
 {
+    if (par < 0) par = ctx->ypar;
     StageArgs a{};
     a.vz = ctx->vz;
     a.rowfac = ctx->rowfac;
@@ -144,32 +146,73 @@ StageArgs stage_args(const cosenu_ctx *ctx, int stage)
     a.pmo = ctx->p.pmo;
     const double ko = 1.0e-1;  // src/nuosc.hpp:60
     a.ko_eps = ctx->p.ko_order == 5 ? -ko / ctx->dz / 64.0 : -ko / ctx->dz / 16.0;
-    a.Y = ctx->Y;
-    a.A = ctx->A;
     a.wait_ns = ctx->wait_ns;
     a.stall = ctx->stall;
-    switch (stage) {
-    case 1: a.X = ctx->Y; a.U = ctx->U0; a.Min = ctx->M[2]; a.Mout = ctx->M[0]; break;
-    case 2: a.X = ctx->U0; a.U = ctx->U1; a.Min = ctx->M[0]; a.Mout = ctx->M[1]; break;
-    case 3: a.X = ctx->U1; a.U = ctx->U0; a.Min = ctx->M[1]; a.Mout = ctx->M[0]; break;
-    case 4: a.X = ctx->U0; a.U = ctx->Y; a.Min = ctx->M[0]; a.Mout = ctx->M[2]; break;
+    double *Y = ctx->Yb[par];
+    a.Y = Y;
+    if (!ctx->fp32) {
+        // FP64 stage values; the accumulator lives in Yb[1] (par is always 0)
+        a.A = ctx->Yb[1];
+        switch (stage) {
+        case 1: a.X = Y; a.U = ctx->U0; a.Min = ctx->M[2]; a.Mout = ctx->M[0]; break;
+        case 2: a.X = ctx->U0; a.U = ctx->U1; a.Min = ctx->M[0]; a.Mout = ctx->M[1]; break;
+        case 3: a.X = ctx->U1; a.U = ctx->U0; a.Min = ctx->M[1]; a.Mout = ctx->M[0]; break;
+        case 4: a.X = ctx->U0; a.U = Y; a.Min = ctx->M[0]; a.Mout = ctx->M[2]; break;
+        }
+    } else {
+        // FP32-bulk increments D1, D2, D3 in U0, U1, U2; the new state goes to
+        // the other FP64 buffer
+        a.T1 = static_cast<const float *>(ctx->U0);
+        a.T2 = static_cast<const float *>(ctx->U1);
+        switch (stage) {
+        case 1: a.X = Y; a.U = ctx->U0; a.Min = ctx->M[2]; a.Mout = ctx->M[0]; break;
+        case 2: a.X = ctx->U0; a.U = ctx->U1; a.Min = ctx->M[0]; a.Mout = ctx->M[1]; break;
+        case 3: a.X = ctx->U1; a.U = ctx->U2; a.Min = ctx->M[1]; a.Mout = ctx->M[0]; break;
+        case 4: a.X = ctx->U2; a.U = ctx->Yb[par ^ 1]; a.Min = ctx->M[0]; a.Mout = ctx->M[2]; break;
+        }
     }
     return a;
 }
 
+void flip(cosenu_ctx *ctx)
+{
+    if (!ctx->fp32) return;
+    ctx->ypar ^= 1;
+    ctx->Y = ctx->Yb[ctx->ypar];
+    ctx->A = ctx->Yb[ctx->ypar ^ 1];
+}
+
+// Launches one stage; after stage 4 of the FP32-bulk form the state is in the
+// other buffer.
 cudaError_t launch_stage(cosenu_ctx *ctx, int stage, cudaStream_t s)
 {
-    StageArgs a = stage_args(ctx, stage);
+    StageArgs a = stage_args(ctx, stage, -1);
+    cudaError_t e;
     if (ctx->use_tma) {
-        const CUtensorMap &mX = stage == 1 ? ctx->mY40 : (stage == 3 ? ctx->mU1_40 : ctx->mU0_40);
         int nblk = std::min(ctx->p.nz / tma_box_tile(),
                             tma_blocks_per_sm(ctx->p.scheme) * ctx->nsm);
-        // stage 3 with FP64 stage values reads U at its own cells in the A slot
-        const CUtensorMap &mA = (stage == 3 && !ctx->fp32) ? ctx->mU0_32 : ctx->mA32;
-        return launch_rk4_stage_tma(mX, ctx->mY32, mA, a, ctx->p.scheme, stage, ctx->fp32,
-                                    ctx->err_flag, nblk, s);
+        const CUtensorMap *mX, *mY, *mA, *mB;
+        if (!ctx->fp32) {
+            // stage 3 reads U at its own cells in the A slot
+            mX = stage == 1 ? &ctx->mYb40[0] : (stage == 3 ? &ctx->mU1_40 : &ctx->mU0_40);
+            mY = &ctx->mY32;
+            mA = stage == 3 ? &ctx->mU0_32 : &ctx->mA32;
+            mB = &ctx->mY32;  // unused
+        } else {
+            // input Y + D with the halo; stage 4 also reads D1, D2 at its own cells
+            mY = &ctx->mYb40[ctx->ypar];
+            mX = stage == 1 ? mY : (stage == 2 ? &ctx->mU0_40 : (stage == 3 ? &ctx->mU1_40
+                                                                             : &ctx->mU2_40));
+            mA = &ctx->mU0_32;
+            mB = &ctx->mU1_32;
+        }
+        e = launch_rk4_stage_tma(*mX, *mY, *mA, *mB, a, ctx->p.scheme, stage, ctx->fp32,
+                                 ctx->err_flag, nblk, s);
+    } else {
+        e = launch_rk4_stage(a, ctx->p.scheme, stage, ctx->tz, ctx->fp32, s);
     }
-    return launch_rk4_stage(a, ctx->p.scheme, stage, ctx->tz, ctx->fp32, s);
+    if (e == cudaSuccess && stage == 4) flip(ctx);
+    return e;
 }
 
 // Reads the device error word; non-zero means a bounded wait in a stage
@@ -199,9 +242,19 @@ cudaError_t launch_steps(cosenu_ctx *ctx, int n, cudaStream_t s)
     return cudaSuccess;
 }
 
-// Captures `n` steps into an executable graph (on a private stream).
+// Captures `n` steps from the current buffer parity into an executable graph
+// (on a private stream); the context's parity is left as it was, since nothing
+// ran yet.
 cudaError_t capture(cosenu_ctx *ctx, int n, cudaGraphExec_t *out)
 {
+    struct Restore {
+        cosenu_ctx *c;
+        int par;
+        ~Restore()
+        {
+            if (c->ypar != par) flip(c);
+        }
+    } restore{ctx, ctx->ypar};
     cudaStream_t cs;
     cudaError_t e = cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking);
     if (e != cudaSuccess) return e;
@@ -247,9 +300,11 @@ int copy_planes_h2d(cosenu_ctx *ctx, double *dst, const double *const *src, int 
 
 void drop_graphs(cosenu_ctx *ctx)
 {
-    if (ctx->g1) cudaGraphExecDestroy(ctx->g1);
-    if (ctx->gN) cudaGraphExecDestroy(ctx->gN);
-    ctx->g1 = ctx->gN = nullptr;
+    for (int k = 0; k < 2; ++k) {
+        if (ctx->g1[k]) cudaGraphExecDestroy(ctx->g1[k]);
+        if (ctx->gN[k]) cudaGraphExecDestroy(ctx->gN[k]);
+        ctx->g1[k] = ctx->gN[k] = nullptr;
+    }
 }
 
 }  // namespace
@@ -366,7 +421,7 @@ int ctx_create(const cosenu_params *pp, cosenu_ctx **out, int layout)
     int rc;
     const size_t plane = (size_t)ctx->cs * sizeof(double);
     const size_t state = plane * NCOMP;
-    const size_t ustate = ctx->fp32 ? state / 2 : state;
+    const size_t ustate = ctx->fp32 ? state / 2 : state;  // U0, U1 (and U2: FP32-bulk)
     // ensemble members may later be re-tiled down to 8-row v tiles
     ctx->mom_nvt_cap = layout == 1 ? (p.nvz + 7) / 8 : ctx->nvt;
     const size_t mom = (size_t)ctx->mom_nvt_cap * NMOM * p.nz * sizeof(double);
@@ -376,11 +431,14 @@ int ctx_create(const cosenu_params *pp, cosenu_ctx **out, int layout)
         cosenu_destroy(ctx);                                                    \
         return rc;                                                              \
     }
-    AL(ctx->Y, state);
-    AL(ctx->A, state);
+    AL(ctx->Yb[0], state);
+    AL(ctx->Yb[1], state);
+    ctx->Y = ctx->Yb[0];
+    ctx->A = ctx->Yb[1];
     AL(ctx->S0, state);
     AL(ctx->U0, ustate);
     AL(ctx->U1, ustate);
+    if (ctx->fp32) AL(ctx->U2, ustate);
     AL(ctx->G, plane);
     AL(ctx->bG, plane);
     for (int k = 0; k < 3; ++k) AL(ctx->M[k], mom);
@@ -406,8 +464,10 @@ int ctx_create(const cosenu_params *pp, cosenu_ctx **out, int layout)
     }
     ctx->stream = ctx->own_stream;
     // zero everything once so ghost pads and unused partials are defined
-    for (void *q : {(void *)ctx->Y, (void *)ctx->A, (void *)ctx->S0, ctx->U0, ctx->U1})
-        cudaMemsetAsync(q, 0, q == ctx->U0 || q == ctx->U1 ? ustate : state, ctx->stream);
+    for (void *q : {(void *)ctx->Yb[0], (void *)ctx->Yb[1], (void *)ctx->S0})
+        cudaMemsetAsync(q, 0, state, ctx->stream);
+    for (void *q : {ctx->U0, ctx->U1, ctx->U2})
+        if (q) cudaMemsetAsync(q, 0, ustate, ctx->stream);
     cudaMemsetAsync(ctx->G, 0, plane, ctx->stream);
     cudaMemsetAsync(ctx->bG, 0, plane, ctx->stream);
     for (int k = 0; k < 3; ++k) cudaMemsetAsync(ctx->M[k], 0, mom, ctx->stream);
@@ -422,13 +482,19 @@ int ctx_create(const cosenu_params *pp, cosenu_ctx **out, int layout)
     }
     cudaMemsetAsync(ctx->err_flag, 0, 64, ctx->stream);
     if (ctx->use_tma) {
-        const int ub = ctx->fp32 ? 4 : 8, bx = tma_box_x(), bt = tma_box_tile();
-        int r = make_state_map(&ctx->mY40, ctx->Y, 8, ctx->ld, p.nvz, ctx->cs, bx);
-        if (!r) r = make_state_map(&ctx->mU0_40, ctx->U0, ub, ctx->ld, p.nvz, ctx->cs, bx);
-        if (!r) r = make_state_map(&ctx->mU1_40, ctx->U1, ub, ctx->ld, p.nvz, ctx->cs, bx);
-        if (!r) r = make_state_map(&ctx->mY32, ctx->Y, 8, ctx->ld, p.nvz, ctx->cs, bt);
-        if (!r) r = make_state_map(&ctx->mA32, ctx->A, 8, ctx->ld, p.nvz, ctx->cs, bt);
+        const int ub = ctx->fp32 ? 4 : 8, bx = tma_box_x(8), bxu = tma_box_x(ub),
+                  bt = tma_box_tile();
+        int r = make_state_map(&ctx->mYb40[0], ctx->Yb[0], 8, ctx->ld, p.nvz, ctx->cs, bx);
+        if (!r) r = make_state_map(&ctx->mYb40[1], ctx->Yb[1], 8, ctx->ld, p.nvz, ctx->cs, bx);
+        if (!r) r = make_state_map(&ctx->mU0_40, ctx->U0, ub, ctx->ld, p.nvz, ctx->cs, bxu);
+        if (!r) r = make_state_map(&ctx->mU1_40, ctx->U1, ub, ctx->ld, p.nvz, ctx->cs, bxu);
+        if (!r) r = make_state_map(&ctx->mY32, ctx->Yb[0], 8, ctx->ld, p.nvz, ctx->cs, bt);
+        if (!r) r = make_state_map(&ctx->mA32, ctx->Yb[1], 8, ctx->ld, p.nvz, ctx->cs, bt);
         if (!r) r = make_state_map(&ctx->mU0_32, ctx->U0, ub, ctx->ld, p.nvz, ctx->cs, bt);
+        if (!r) r = make_state_map(&ctx->mU1_32, ctx->U1, ub, ctx->ld, p.nvz, ctx->cs, bt);
+        if (!r && ctx->U2)
+            r = make_state_map(&ctx->mU2_40, ctx->U2, ub, ctx->ld, p.nvz, ctx->cs, bxu);
+        if (!ctx->U2) ctx->mU2_40 = ctx->mU1_40;  // unused in FP64
         if (!r && tma_prepare() != cudaSuccess) r = -2;
         if (r) {
             // no tensor-map support: fall back to the register-tiled kernel
@@ -444,8 +510,21 @@ int ctx_create(const cosenu_params *pp, cosenu_ctx **out, int layout)
     return COSENU_OK;
 }
 
-StageArgs ctx_stage_args(const cosenu_ctx *ctx, int stage) { return stage_args(ctx, stage); }
+StageArgs ctx_stage_args(const cosenu_ctx *ctx, int stage, int par)
+{
+    return stage_args(ctx, stage, par);
+}
 int ctx_prepare_state(cosenu_ctx *ctx) { return prepare_state(ctx); }
+void ctx_flip(cosenu_ctx *ctx) { flip(ctx); }
+
+int ctx_normalise_parity(cosenu_ctx *ctx)
+{
+    if (ctx->ypar == 0) return COSENU_OK;
+    CK(cudaMemcpyAsync(ctx->Yb[0], ctx->Yb[1], (size_t)ctx->cs * 8 * NCOMP,
+                       cudaMemcpyDeviceToDevice, ctx->stream));
+    flip(ctx);
+    return COSENU_OK;
+}
 
 int ctx_set_tiling(cosenu_ctx *ctx, int tz, int tv)
 {
@@ -475,7 +554,7 @@ int cosenu_destroy(cosenu_ctx *ctx)
     DeviceGuard dg(ctx->p.device);
     if (ctx->stream) cudaStreamSynchronize(ctx->stream);
     drop_graphs(ctx);
-    void *bufs[] = {ctx->Y, ctx->A, ctx->S0, ctx->U0, ctx->U1, ctx->G, ctx->bG, ctx->M[0],
+    void *bufs[] = {ctx->Yb[0], ctx->Yb[1], ctx->S0, ctx->U0, ctx->U1, ctx->U2, ctx->G, ctx->bG, ctx->M[0],
                     ctx->M[1], ctx->M[2], ctx->vz, ctx->rowfac, ctx->Hm, ctx->diag_part,
                     ctx->diag_out, ctx->pee, ctx->tmp, ctx->err_flag};
     for (void *b : bufs)
@@ -711,14 +790,23 @@ int cosenu_step(cosenu_ctx *ctx, int nsteps)
     if (!ctx->use_graphs || nsteps == 1) {
         CK(launch_steps(ctx, nsteps, ctx->stream));
     } else {
-        if (!ctx->g1) CK(capture(ctx, 1, &ctx->g1));
-        if (nsteps >= GRAPH_CHUNK && !ctx->gN) CK(capture(ctx, GRAPH_CHUNK, &ctx->gN));
+        // graphs start from a given buffer parity (FP32-bulk alternates it;
+        // GRAPH_CHUNK is even, so the long graph leaves it unchanged)
         int n = nsteps;
-        while (n >= GRAPH_CHUNK) {
-            CK(cudaGraphLaunch(ctx->gN, ctx->stream));
-            n -= GRAPH_CHUNK;
+        if (n >= GRAPH_CHUNK) {
+            cudaGraphExec_t &g = ctx->gN[ctx->ypar];
+            if (!g) CK(capture(ctx, GRAPH_CHUNK, &g));
+            while (n >= GRAPH_CHUNK) {
+                CK(cudaGraphLaunch(g, ctx->stream));
+                n -= GRAPH_CHUNK;
+            }
         }
-        while (n-- > 0) CK(cudaGraphLaunch(ctx->g1, ctx->stream));
+        while (n-- > 0) {
+            cudaGraphExec_t &g = ctx->g1[ctx->ypar];
+            if (!g) CK(capture(ctx, 1, &g));
+            CK(cudaGraphLaunch(g, ctx->stream));
+            flip(ctx);
+        }
     }
     ctx->steps += nsteps;
     return COSENU_OK;

@@ -28,10 +28,11 @@ enum Flags { F_VAC = 1, F_MAT = 2, F_COLL = 4, F_ADVEC_OFF = 8 };
 
 // Arguments of one RK4 stage launch (passed by value).
 struct StageArgs {
-    const void *X;       // stage input (U or Y), TIN, with ghosts
-    const double *Y;     // RK4 base state (stages 2, 3)
-    double *A;           // RK4 accumulator
-    void *U;             // stage output, TOUT (U', U'' or the new Y)
+    const void *X;       // stage input, TIN, with ghosts: U or Y (FP64); D or Y (FP32-bulk)
+    const double *Y;     // RK4 base state (FP64 stages 2, 3; FP32-bulk stages 2-4, with ghosts)
+    double *A;           // RK4 accumulator (FP64)
+    void *U;             // stage output, TOUT (U', U'' or the new Y; D1, D2, D3 or the new Y)
+    const float *T1, *T2;  // FP32-bulk stage 4: the increments D1, D2 at its own cells
     const double *Min;   // [nvt][6][nz] per-v-tile moments of X
     double *Mout;        // [nvt][6][nz] per-v-tile moments of U
     const double *vz;    // [nvz] velocities
@@ -77,13 +78,23 @@ inline int padded_ld(int nz) { return ((nz + 2 * HP + 15) / 16) * 16; }
 //            A   = Y + (U - Y)/3 + 2 (U' - Y)/3 + dt/3 k3
 //            (reads U', Y and U at its own cells; writes U'' over U, and A)
 //   stage 4: Y   = A + dt/6 k4                          (reads U'', A, writes Y)
-// With FP32 stage values a difference would carry FP32 rounding into the FP64
-// accumulator, so A is updated at every stage as the reference's vectorize
-// does (src/nuosc.hpp:281-318).  a_deferred: this stage uses the FP64 form.
-template <int STAGE, class TIN, class TOUT>
-__host__ __device__ constexpr bool a_deferred()
+//
+// FP32-bulk keeps the base state Y in FP64 and stores the stage increments,
+// not the stage values, in FP32: D1 = dt/2 k1, D2 = dt/2 k2, D3 = dt k3.  They
+// are small, so FP32 holds them to ~6e-8 of dt*k rather than of U, and each
+// stage reads its input as Y + D in FP64:
+//   stage 1: D1 = dt/2 k1(Y)                             (reads Y, writes D1)
+//   stage 2: D2 = dt/2 k2(Y + D1)                        (reads Y, D1, writes D2)
+//   stage 3: D3 = dt k3(Y + D2)                          (reads Y, D2, writes D3)
+//   stage 4: Y' = Y + (D1 + 2 D2 + D3)/3 + dt/6 k4(Y + D3)
+//            (reads Y, D3, and D1, D2 at its own cells; writes Y')
+// 576 B per cell-update.  Stage 4 reads Y around its cells while it writes the
+// new state, so Y' goes to the second FP64 buffer and the two swap roles every
+// step.  inc_form: a launch of this form (an FP32 operand is involved).
+template <class TIN, class TOUT>
+__host__ __device__ constexpr bool inc_form()
 {
-    return (STAGE == 1 && sizeof(TOUT) == 8) || ((STAGE == 2 || STAGE == 3) && sizeof(TIN) == 8);
+    return sizeof(TIN) == 4 || sizeof(TOUT) == 4;
 }
 
 }  // namespace cosenu

@@ -6,8 +6,9 @@
 // did not plan for, and cudaMalloc/cudaFree can synchronise the device in the
 // middle of a latency-sensitive loop.  This entry point lets such a caller
 // advance a state it already holds in device memory.  Its working memory
-// (a padded copy of the state with ghost cells, the RK4 stage buffers U0, U1,
-// A, the velocity-moment partials and the per-row tables) lives in one
+// (a padded copy of the state with ghost cells, the RK4 stage buffers -- U0,
+// U1, A in FP64; a second state buffer and the increments D1, D2, D3 in
+// FP32-bulk --, the velocity-moment partials and the per-row tables) lives in one
 // file-scope device array of fixed size, NOALLOC_SCRATCH_DOUBLES doubles
 // (20.5 MB), which every GPU that loads this library holds until the process
 // exits.
@@ -195,8 +196,14 @@ extern "C" int cosenu_step_noalloc(const cosenu_params *pp, double *const state[
     }
     cudaStream_t s = (cudaStream_t)stream;
     const long long cs = plane;
-    double *Y = base, *A = base + 3 * NCOMP * cs;
+    const int fp32 = p.precision == COSENU_FP32_BULK;
+    // FP64: Y, stage values U0, U1, accumulator A.  FP32-bulk: two state
+    // buffers Y, Y2 (the new state goes to the other one each step) and the
+    // FP32 increments D1, D2, D3.
+    double *Y = base, *A = base + 3 * NCOMP * cs, *Y2 = base + NCOMP * cs;
     void *U0 = base + NCOMP * cs, *U1 = base + 2 * NCOMP * cs;
+    float *D1 = reinterpret_cast<float *>(base + 2 * NCOMP * cs);
+    float *D2 = D1 + NCOMP * cs, *D3 = D2 + NCOMP * cs;
     double *M[3] = {base + 4 * NCOMP * cs, base + 4 * NCOMP * cs + mom, base + 4 * NCOMP * cs + 2 * mom};
     double *vz = base + 4 * NCOMP * cs + 3 * mom, *rowfac = vz + p.nvz, *Hm = rowfac + p.nvz;
     const size_t used = (size_t)((Hm + p.nz) - base) * sizeof(double);
@@ -247,19 +254,33 @@ extern "C" int cosenu_step_noalloc(const cosenu_params *pp, double *const state[
     a.ko_eps = p.ko_order == 5 ? -ko / dz / 64.0 : -ko / dz / 16.0;
     a.Y = Y;
     a.A = A;
-    const int fp32 = p.precision == COSENU_FP32_BULK;
+    a.T1 = D1;
+    a.T2 = D2;
+    double *ycur = Y, *ynext = Y2;
     for (int it = 0; it < nsteps; ++it) {
         for (int st = 1; st <= 4; ++st) {
-            switch (st) {
-            case 1: a.X = Y; a.U = U0; a.Min = M[2]; a.Mout = M[0]; break;
-            case 2: a.X = U0; a.U = U1; a.Min = M[0]; a.Mout = M[1]; break;
-            case 3: a.X = U1; a.U = U0; a.Min = M[1]; a.Mout = M[0]; break;
-            case 4: a.X = U0; a.U = Y; a.Min = M[0]; a.Mout = M[2]; break;
+            if (!fp32) {
+                switch (st) {
+                case 1: a.X = Y; a.U = U0; a.Min = M[2]; a.Mout = M[0]; break;
+                case 2: a.X = U0; a.U = U1; a.Min = M[0]; a.Mout = M[1]; break;
+                case 3: a.X = U1; a.U = U0; a.Min = M[1]; a.Mout = M[0]; break;
+                case 4: a.X = U0; a.U = Y; a.Min = M[0]; a.Mout = M[2]; break;
+                }
+            } else {
+                a.Y = ycur;
+                switch (st) {
+                case 1: a.X = ycur; a.U = D1; a.Min = M[2]; a.Mout = M[0]; break;
+                case 2: a.X = D1; a.U = D2; a.Min = M[0]; a.Mout = M[1]; break;
+                case 3: a.X = D2; a.U = D3; a.Min = M[1]; a.Mout = M[0]; break;
+                case 4: a.X = D3; a.U = ynext; a.Min = M[0]; a.Mout = M[2]; break;
+                }
             }
             if ((e = launch_rk4_stage(a, p.scheme, st, tz, fp32, s)) != cudaSuccess)
                 return done(COSENU_ERR_CUDA, "stage", e);
         }
+        if (fp32) std::swap(ycur, ynext);
     }
+    Y = ycur;
     for (int c = 0; c < NCOMP; ++c) {
         e = cudaMemcpy2DAsync(state[c], (size_t)ld * 8, Y + c * cs + HP, (size_t)ldp * 8,
                               (size_t)p.nz * 8, p.nvz, cudaMemcpyDeviceToDevice, s);

@@ -44,13 +44,17 @@ namespace tma {
 
 constexpr int TZ = 32;           // cells per tile (one warp lane each)
 constexpr int HALO = 4;          // cells each side in the input box
-constexpr int XW = TZ + 2 * HALO;
+// Width of an input box row: the tile plus HALO cells each side, rounded up so
+// that the row is a multiple of 16 bytes (TMA) and the component rows of one
+// v row start in distinct shared-memory banks: the edge faces of a row read
+// the same cell of all 8 components at once (42 doubles = 84 words: banks
+// 0, 20, 8, 28, ... for components 0..7; 44 floats = 44 words: 0, 12, 24, ...).
+template <class T> constexpr int xw() { return sizeof(T) == 8 ? 42 : 44; }
 constexpr int R = 8;             // rows per chunk = consumer warps
 constexpr int NCONS = R * 32;    // consumer threads
 constexpr int NTHR = NCONS + 32; // + producer warp
-// tensor maps per ensemble member: Y, U0, U1 input boxes (with halo), then
-// the Y, A and U0 tile boxes
-constexpr int NMAP = 6;
+// tensor maps per ensemble member (MapIdx lists them)
+constexpr int NMAP = 7;
 #define TMA_MAX_NVZ 1024
 
 __device__ __forceinline__ uint32_t smem_u32(const void *p)
@@ -152,15 +156,33 @@ __device__ __forceinline__ void consumer_sync()
     asm volatile("bar.sync 1, %0;" ::"n"(NCONS) : "memory");
 }
 
-template <class TIN, int STAGE> struct Layout {
+// One ring buffer holds, for R rows, boxes laid out [row][component][cell]
+// (the tensor maps put components before rows): the input box X, then Y, then
+// the own-cell tiles A (and B).
+template <class TIN, class TOUT, int STAGE> struct Layout {
+    static constexpr bool INC = inc_form<TIN, TOUT>();
+    static constexpr int XW = xw<TIN>();
     static constexpr int XB = NCOMP * R * XW * (int)sizeof(TIN);
-    // which of Y and A each stage reads (a_deferred, common.cuh).  Stage 3
-    // with FP64 stage values loads U (its own cells, about to be overwritten
-    // by U'') into the A slot instead of A.
-    static constexpr bool FP64U = sizeof(TIN) == 8;
-    static constexpr int YB = (STAGE == 2 || STAGE == 3) ? NCOMP * R * TZ * 8 : 0;
-    static constexpr int AB = (STAGE >= 3 || (STAGE == 2 && !FP64U)) ? NCOMP * R * TZ * 8 : 0;
+    // Y: FP64 stages 2-3 read it at their own cells; FP32-bulk stages 2-4 read
+    // it with the halo (their input is Y + D)
+    static constexpr int YW =
+        INC ? (STAGE >= 2 ? xw<double>() : 0) : ((STAGE == 2 || STAGE == 3) ? TZ : 0);
+    static constexpr int YB = NCOMP * R * YW * 8;
+    // FP64 stage 3: U at its own cells (about to be overwritten by U''); stage
+    // 4: A.  FP32-bulk stage 4: D1 then D2 at its own cells.
+    static constexpr int AB = INC ? (STAGE == 4 ? 2 * NCOMP * R * TZ * 4 : 0)
+                                  : (STAGE >= 3 ? NCOMP * R * TZ * 8 : 0);
     static constexpr int BUF = ((XB + YB + AB) + 127) / 128 * 128;
+};
+
+// Index of each operand's tensor map among a member's NMAP maps (ensembles).
+// FP64:      0 Y (halo box), 1 U0 (halo), 2 U1 (halo), 3 Y (tile), 4 A (tile), 5 U0 (tile)
+// FP32-bulk: 0 current Y (halo), 1 D1 (halo), 2 D2 (halo), 3 D2 (tile), 5 D1 (tile), 6 D3 (halo)
+template <bool INC, int STAGE> struct MapIdx {
+    static constexpr int X = STAGE == 1 ? 0 : (STAGE == 3 ? 2 : (INC && STAGE == 4 ? 6 : 1));
+    static constexpr int Y = INC ? 0 : 3;
+    static constexpr int A = INC ? 5 : (STAGE == 3 ? 5 : 4);
+    static constexpr int B = 3;
 };
 
 }  // namespace tma
@@ -199,16 +221,23 @@ __device__ __forceinline__ void row_values(double v0, double dv, double dz, int 
     }
 }
 
-template <int SCHEME, bool GEN, int STAGE, class TC, class TIN, class TOUT, int NBUF, bool BATCHED,
-          int MINB>
+// TIN: type of the streamed stage input (FP64: the stage value U or Y;
+// FP32-bulk: Y at stage 1, the increment D after).  TOUT: type of the output
+// (FP64: U', U'' or Y; FP32-bulk: D1, D2, D3, then the new Y).  The
+// right-hand side is evaluated in FP64 in both forms, except the FP32-bulk
+// WENO7 weights and candidates (FP32 on FP64 stencil differences).
+template <int SCHEME, bool GEN, int STAGE, class TIN, class TOUT, int NBUF, bool BATCHED, int MINB>
 __global__ void __launch_bounds__(tma::NTHR, MINB)
     rk4_stage_tma_kernel(const __grid_constant__ CUtensorMap mX,
                          const __grid_constant__ CUtensorMap mY,
                          const __grid_constant__ CUtensorMap mA,
+                         const __grid_constant__ CUtensorMap mB,
                          const __grid_constant__ StageArgs a0, int *err, const BatchDev bd)
 {
     using namespace tma;
-    using L = Layout<TIN, STAGE>;
+    using L = Layout<TIN, TOUT, STAGE>;
+    using MI = MapIdx<L::INC, STAGE>;
+    constexpr bool INC = L::INC;
     extern __shared__ __align__(1024) unsigned char smem[];
     uint64_t *full = reinterpret_cast<uint64_t *>(smem + NBUF * L::BUF);
     uint64_t *empty = full + NBUF;
@@ -247,20 +276,19 @@ __global__ void __launch_bounds__(tma::NTHR, MINB)
                 int4 nxt = cur;
                 if (BATCHED && has_next) nxt = bd.table[t + t_step];
                 const int inst = BATCHED ? cur.x : 0, zt = BATCHED ? cur.y : t;
-                constexpr int MA = (STAGE == 3 && a_deferred<STAGE, TIN, TOUT>()) ? 5 : 4;
-                const CUtensorMap *px =
-                    BATCHED ? &bd.maps[inst * NMAP + (STAGE == 1 ? 0 : (STAGE == 3 ? 2 : 1))]
-                            : &mX;
-                const CUtensorMap *py = BATCHED ? &bd.maps[inst * NMAP + 3] : &mY;
-                const CUtensorMap *pa = BATCHED ? &bd.maps[inst * NMAP + MA] : &mA;
+                const CUtensorMap *px = BATCHED ? &bd.maps[inst * NMAP + MI::X] : &mX;
+                const CUtensorMap *py = BATCHED ? &bd.maps[inst * NMAP + MI::Y] : &mY;
+                const CUtensorMap *pa = BATCHED ? &bd.maps[inst * NMAP + MI::A] : &mA;
+                const CUtensorMap *pb = BATCHED ? &bd.maps[inst * NMAP + MI::B] : &mB;
                 const int z0 = zt * TZ;
                 const int nch = ((BATCHED ? cur.w : a0.nvz) + R - 1) / R;
                 for (int ch = 0; ch < nch; ++ch, ++it) {
                     if (BATCHED && ch == 0 && has_next && nxt.x != inst) {
                         const CUtensorMap *m = &bd.maps[nxt.x * NMAP];
-                        tma::prefetch_map(&m[STAGE == 1 ? 0 : (STAGE == 3 ? 2 : 1)]);
-                        if (L::YB) tma::prefetch_map(&m[3]);
-                        if (L::AB) tma::prefetch_map(&m[MA]);
+                        tma::prefetch_map(&m[MI::X]);
+                        if (L::YB) tma::prefetch_map(&m[MI::Y]);
+                        if (L::AB) tma::prefetch_map(&m[MI::A]);
+                        if (INC && L::AB) tma::prefetch_map(&m[MI::B]);
                     }
                     const int b = it % NBUF;
                     if (it >= (uint32_t)NBUF &&
@@ -270,10 +298,18 @@ __global__ void __launch_bounds__(tma::NTHR, MINB)
                     }
                     unsigned char *buf = smem + b * L::BUF;
                     tma::mbar_expect_tx(&full[b], L::XB + L::YB + L::AB);
-                    tma::tma_load_3d(buf, px, HP + z0 - HALO, ch * R, 0, &full[b]);
-                    if (L::YB) tma::tma_load_3d(buf + L::XB, py, HP + z0, ch * R, 0, &full[b]);
-                    if (L::AB)
-                        tma::tma_load_3d(buf + L::XB + L::YB, pa, HP + z0, ch * R, 0, &full[b]);
+                    // coordinates: (cell, component 0, first row of the chunk)
+                    tma::tma_load_3d(buf, px, HP + z0 - HALO, 0, ch * R, &full[b]);
+                    if (L::YB)
+                        tma::tma_load_3d(buf + L::XB, py, HP + z0 - (INC ? HALO : 0), 0, ch * R,
+                                         &full[b]);
+                    if (L::AB && !INC)
+                        tma::tma_load_3d(buf + L::XB + L::YB, pa, HP + z0, 0, ch * R, &full[b]);
+                    if (L::AB && INC) {
+                        tma::tma_load_3d(buf + L::XB + L::YB, pa, HP + z0, 0, ch * R, &full[b]);
+                        tma::tma_load_3d(buf + L::XB + L::YB + L::AB / 2, pb, HP + z0, 0, ch * R,
+                                         &full[b]);
+                    }
                 }
                 cur = nxt;
             }
@@ -338,8 +374,6 @@ __global__ void __launch_bounds__(tma::NTHR, MINB)
                 mnext = an.Min[(long long)(tid / TZ) * an.nz + zn * TZ + tid % TZ];
         }
         double macc[NMOM] = {0, 0, 0, 0, 0, 0};
-        const double M0A = s_mom[0][lane], M0B = s_mom[1][lane], M0C = s_mom[2][lane],
-                     M1A = s_mom[3][lane], M1B = s_mom[4][lane], M1C = s_mom[5][lane];
 
         for (int ch = 0; ch < nch; ++ch, ++it) {
             const int b = it % NBUF;
@@ -348,50 +382,63 @@ __global__ void __launch_bounds__(tma::NTHR, MINB)
             const int vr = valid ? v : a.nvz - 1;
             double vzv, fac;
             row_values<SCHEME>(a.v0, a.dv, a.dz, a.fd_advec, vr, vzv, fac);
-            const TC factor = (TC)fac;
+            const double factor = fac;
             const bool landed = tma::mbar_wait(&full[b], (it / NBUF) & 1, err, 2, a0.wait_ns);
             const unsigned char *buf = smem + b * L::BUF;
-            const TIN *xrow = reinterpret_cast<const TIN *>(buf) + warp * XW + HALO;
-            const TIN *xs = xrow + lane;
-            const double *ys = reinterpret_cast<const double *>(buf + L::XB) + warp * TZ + lane;
-            const double *as = reinterpret_cast<const double *>(buf + L::XB + L::YB) + warp * TZ + lane;
+            // this warp's row of component 0 in the input box (HALO cells each
+            // side); the row's components are XW cells apart
+            constexpr int XW = L::XW, YW = L::YW;
+            const TIN *xrow = reinterpret_cast<const TIN *>(buf) + warp * (NCOMP * XW) + HALO;
+            const double *yrow = reinterpret_cast<const double *>(buf + L::XB) +
+                                 warp * (NCOMP * YW) + (INC ? HALO : 0);
+            // the stage input at cell j of this row (j in [-HALO, TZ + HALO))
+            auto in = [&](int q, int j) -> double {
+                if constexpr (INC && STAGE >= 2)
+                    return yrow[q * YW + j] + (double)xrow[q * XW + j];
+                else
+                    return (double)xrow[q * XW + j];
+            };
+            // upwind WENO7 face of component q about cell j, stencil direction dir
+            auto face = [&](int q, int j, int dir) -> double {
+                if constexpr (INC) {
+                    const double u = in(q, j);
+                    return u + (double)weno7_corr(
+                                   (float)(in(q, j - 3 * dir) - u), (float)(in(q, j - 2 * dir) - u),
+                                   (float)(in(q, j - dir) - u), (float)(in(q, j + dir) - u),
+                                   (float)(in(q, j + 2 * dir) - u), (float)(in(q, j + 3 * dir) - u));
+                } else {
+                    return weno7_face(in(q, j - 3 * dir), in(q, j - 2 * dir), in(q, j - dir),
+                                      in(q, j), in(q, j + dir), in(q, j + 2 * dir),
+                                      in(q, j + 3 * dir));
+                }
+            };
 
-            TC c[NCOMP], o[NCOMP], ko[NCOMP];
-            double x0[NCOMP];
+            double c[NCOMP], o[NCOMP], ko[NCOMP];
 #pragma unroll
-            for (int q = 0; q < NCOMP; ++q) {
-                x0[q] = (double)xs[q * (R * XW)];
-                c[q] = (TC)x0[q];
-            }
+            for (int q = 0; q < NCOMP; ++q) c[q] = in(q, lane);
             if (SCHEME == FV) {
                 // upwind flux difference (rhs_fv.hpp:143-162): this lane's face
                 // and its neighbour's; lanes 0-7 first build the row's edge faces
                 const int dir = (vzv >= 0.0) ? 1 : -1;
-                TC edge = TC(0);
-                if (advec && lane < NCOMP) {
-                    const TIN *pe = xrow + lane * (R * XW) + (dir > 0 ? -1 : TZ);
-                    edge = weno7_face((TC)pe[-3 * dir], (TC)pe[-2 * dir], (TC)pe[-dir], (TC)pe[0],
-                                      (TC)pe[dir], (TC)pe[2 * dir], (TC)pe[3 * dir]);
-                }
+                double edge = 0.0;
+                if (advec && lane < NCOMP) edge = face(lane, dir > 0 ? -1 : TZ, dir);
                 const int src = min(max(lane - dir, 0), TZ - 1);
 #pragma unroll
                 for (int q = 0; q < NCOMP; ++q) {
-                    TC adv = TC(0);
+                    double adv = 0.0;
                     if (advec) {
-                        const TIN *p = xs + q * (R * XW);
-                        const TC fown = weno7_face((TC)p[-3 * dir], (TC)p[-2 * dir], (TC)p[-dir],
-                                                   (TC)p[0], (TC)p[dir], (TC)p[2 * dir],
-                                                   (TC)p[3 * dir]);
-                        TC fnb = __shfl_sync(0xffffffffu, fown, src);
-                        const TC e = __shfl_sync(0xffffffffu, edge, q);
+                        const double fown = face(q, lane, dir);
+                        double fnb = __shfl_sync(0xffffffffu, fown, src);
+                        const double e = __shfl_sync(0xffffffffu, edge, q);
                         if ((dir > 0 && lane == 0) || (dir < 0 && lane == TZ - 1)) fnb = e;
                         if (open_bc) {
                             // flux ghosts under OPEN_BC (updateBufferZone on rflux/lflux,
                             // rhs_fv.hpp:118-119): rflux[-1] = rflux[0],
                             // lflux[nz] = 2 lflux[nz-1] - lflux[nz-2]
-                            const TC fm1 = __shfl_sync(0xffffffffu, fown, lane > 0 ? lane - 1 : 0);
+                            const double fm1 =
+                                __shfl_sync(0xffffffffu, fown, lane > 0 ? lane - 1 : 0);
                             if (dir > 0 && z == 0) fnb = fown;
-                            if (dir < 0 && z == a.nz - 1) fnb = fown * TC(2) - fm1;
+                            if (dir < 0 && z == a.nz - 1) fnb = fown * 2.0 - fm1;
                         }
                         adv = dir > 0 ? factor * (fown - fnb) : factor * (fnb - fown);
                     }
@@ -400,18 +447,18 @@ __global__ void __launch_bounds__(tma::NTHR, MINB)
                 if (a.flags & F_VAC) {
                     // read where used: batched, a is in shared memory and a
                     // per-tile copy would hold registers across the chunk loop
-                    const TC pmo = (TC)a.pmo, ct = (TC)a.ct, st = (TC)a.st;
-                    o[EE] += TC(-2) * st * c[EXI] * pmo;
-                    o[XX] += TC(2) * st * c[EXI] * pmo;
-                    o[EXR] += TC(-2) * ct * c[EXI] * pmo;
-                    o[EXI] += (TC(2) * ct * c[EXR] + st * (c[EE] - c[XX])) * pmo;
-                    o[BEE] += TC(-2) * st * c[BEXI] * pmo;
-                    o[BXX] += TC(2) * st * c[BEXI] * pmo;
-                    o[BEXR] += TC(-2) * ct * c[BEXI] * pmo;
-                    o[BEXI] += (TC(2) * ct * c[BEXR] + st * (c[BEE] - c[BXX])) * pmo;
+                    const double pmo = a.pmo, ct = a.ct, st = a.st;
+                    o[EE] += -2.0 * st * c[EXI] * pmo;
+                    o[XX] += 2.0 * st * c[EXI] * pmo;
+                    o[EXR] += -2.0 * ct * c[EXI] * pmo;
+                    o[EXI] += (2.0 * ct * c[EXR] + st * (c[EE] - c[XX])) * pmo;
+                    o[BEE] += -2.0 * st * c[BEXI] * pmo;
+                    o[BXX] += 2.0 * st * c[BEXI] * pmo;
+                    o[BEXR] += -2.0 * ct * c[BEXI] * pmo;
+                    o[BEXI] += (2.0 * ct * c[BEXR] + st * (c[BEE] - c[BXX])) * pmo;
                 }
                 if (a.flags & F_MAT) {
-                    const TC hm = (TC)a.Hm[z];
+                    const double hm = a.Hm[z];
                     o[EXR] += hm * c[EXI];
                     o[EXI] += -hm * c[EXR];
                     o[BEXR] += -hm * c[BEXI];
@@ -420,61 +467,65 @@ __global__ void __launch_bounds__(tma::NTHR, MINB)
             } else {
                 // FD: vacuum, matter, advection, (collective below), dissipation
 #pragma unroll
-                for (int q = 0; q < NCOMP; ++q) o[q] = TC(0);
+                for (int q = 0; q < NCOMP; ++q) o[q] = 0.0;
                 if (a.flags & F_VAC) {
                     // read where used: batched, a is in shared memory and a
                     // per-tile copy would hold registers across the chunk loop
-                    const TC pmo = (TC)a.pmo, ct = (TC)a.ct, st = (TC)a.st;
-                    o[EE] = -pmo * TC(2) * st * c[EXI];
-                    o[XX] = pmo * TC(2) * st * c[EXI];
-                    o[EXR] = -pmo * TC(2) * ct * c[EXI];
-                    o[EXI] = pmo * (TC(2) * ct * c[EXR] + st * (c[EE] - c[XX]));
-                    o[BEE] = -pmo * TC(2) * st * c[BEXI];
-                    o[BXX] = pmo * TC(2) * st * c[BEXI];
-                    o[BEXR] = -pmo * TC(2) * ct * c[BEXI];
-                    o[BEXI] = pmo * (TC(2) * ct * c[BEXR] + st * (c[BEE] - c[BXX]));
+                    const double pmo = a.pmo, ct = a.ct, st = a.st;
+                    o[EE] = -pmo * 2.0 * st * c[EXI];
+                    o[XX] = pmo * 2.0 * st * c[EXI];
+                    o[EXR] = -pmo * 2.0 * ct * c[EXI];
+                    o[EXI] = pmo * (2.0 * ct * c[EXR] + st * (c[EE] - c[XX]));
+                    o[BEE] = -pmo * 2.0 * st * c[BEXI];
+                    o[BXX] = pmo * 2.0 * st * c[BEXI];
+                    o[BEXR] = -pmo * 2.0 * ct * c[BEXI];
+                    o[BEXI] = pmo * (2.0 * ct * c[BEXR] + st * (c[BEE] - c[BXX]));
                 }
                 if (a.flags & F_MAT) {
-                    const TC hm = (TC)a.Hm[z];
+                    const double hm = a.Hm[z];
                     o[EXR] += hm * c[EXI];
                     o[EXI] += -hm * c[EXR];
                     o[BEXR] += -hm * c[BEXI];
                     o[BEXI] += hm * c[BEXR];
                 }
                 const int sv = (vzv > 0.0) - (vzv < 0.0);
-                const TC ko_eps = (TC)a.ko_eps;
+                const double ko_eps = a.ko_eps;
                 // one pass over each stencil: advection now, dissipation kept
                 // for after the collective term (the reference's order)
 #pragma unroll
                 for (int q = 0; q < NCOMP; ++q) {
-                    const TIN *p = xs + q * (R * XW);
-                    const TC m2 = (TC)p[-2], m1 = (TC)p[-1], p1 = (TC)p[1], p2 = (TC)p[2];
+                    const double m2 = in(q, lane - 2), m1 = in(q, lane - 1), p1 = in(q, lane + 1),
+                                 p2 = in(q, lane + 2);
                     if (advec) {
-                        TC adv;
+                        double adv;
                         if (!GEN || a.fd_advec == 0) {
-                            adv = factor * ((m2 - p2) - TC(8) * (m1 - p1));
+                            adv = factor * ((m2 - p2) - 8.0 * (m1 - p1));
                         } else if (a.fd_advec == 1) {
-                            adv = factor * (TC(-4) * (TC)p[-3 * sv] + TC(18) * (TC)p[-2 * sv] -
-                                            TC(36) * (TC)p[-sv] + TC(22) * c[q]);
+                            adv = factor * (-4.0 * in(q, lane - 3 * sv) + 18.0 * in(q, lane - 2 * sv) -
+                                            36.0 * in(q, lane - sv) + 22.0 * c[q]);
                         } else {
-                            adv = factor * ((TC)p[-3 * sv] - TC(6) * (TC)p[-2 * sv] +
-                                            TC(18) * (TC)p[-sv] - TC(10) * c[q] - TC(3) * (TC)p[sv]);
+                            adv = factor * (in(q, lane - 3 * sv) - 6.0 * in(q, lane - 2 * sv) +
+                                            18.0 * in(q, lane - sv) - 10.0 * c[q] -
+                                            3.0 * in(q, lane + sv));
                         }
                         o[q] += adv;
                     }
                     if (GEN && a.ko_order == 5)
-                        ko[q] = ko_eps * ((TC)p[-3] + (TC)p[3] - TC(6) * (m2 + p2) +
-                                          TC(15) * (m1 + p1) - TC(20) * c[q]);
+                        ko[q] = ko_eps * (in(q, lane - 3) + in(q, lane + 3) - 6.0 * (m2 + p2) +
+                                          15.0 * (m1 + p1) - 20.0 * c[q]);
                     else
-                        ko[q] = ko_eps * (m2 + p2 - TC(4) * (m1 + p1) + TC(6) * c[q]);
+                        ko[q] = ko_eps * (m2 + p2 - 4.0 * (m1 + p1) + 6.0 * c[q]);
                 }
             }
             if (coll) {
-                const TC mudv = (TC)(a.mu * a.dv);
-                const TC SA = (TC)(M0A - vzv * M1A), SB = (TC)(M0B - vzv * M1B),
-                         SC = (TC)(M0C - vzv * M1C);
-                const TC Iee = TC(2) * (c[EXR] * SA - c[EXI] * SB);
-                const TC Ibee = TC(2) * (c[BEXR] * SA + c[BEXI] * SB);
+                // this tile's input moments, read where used (they stay in
+                // shared memory until the tile epilogue replaces them)
+                const double mudv = a.mu * a.dv;
+                const double SA = s_mom[0][lane] - vzv * s_mom[3][lane],
+                             SB = s_mom[1][lane] - vzv * s_mom[4][lane],
+                             SC = s_mom[2][lane] - vzv * s_mom[5][lane];
+                const double Iee = 2.0 * (c[EXR] * SA - c[EXI] * SB);
+                const double Ibee = 2.0 * (c[BEXR] * SA + c[BEXI] * SB);
                 o[EE] += mudv * Iee;
                 o[XX] += mudv * (-Iee);
                 o[EXR] += mudv * ((c[XX] - c[EE]) * SA + c[EXI] * SC);
@@ -489,31 +540,52 @@ __global__ void __launch_bounds__(tma::NTHR, MINB)
                 for (int q = 0; q < NCOMP; ++q) o[q] += ko[q];
             }
 
-            // stage combine (a_deferred, common.cuh: with FP64 stage values A
-            // is written once, by stage 3, from U (in the A slot), U' and Y)
-            constexpr bool AD = a_deferred<STAGE, TIN, TOUT>();
+            // stage combine.  FP64 (stage values, A written once by stage 3 from
+            // U in the A slot, U' and Y) or FP32-bulk (increments, common.cuh).
             const double dt = a.dt;
+            // own-cell tiles: [row][component][TZ cells]
+            const double *ys =
+                reinterpret_cast<const double *>(buf + L::XB) + warp * (NCOMP * TZ) + lane;
+            const double *as =
+                reinterpret_cast<const double *>(buf + L::XB + L::YB) + warp * (NCOMP * TZ) + lane;
+            const float *d1s =
+                reinterpret_cast<const float *>(buf + L::XB + L::YB) + warp * (NCOMP * TZ) + lane;
             TOUT u[NCOMP];
-            double anew[NCOMP];
+            double anew[NCOMP];  // FP64 stage 3: the accumulator
+            double um[NCOMP];    // the output as a stage value (for the moments)
 #pragma unroll
             for (int q = 0; q < NCOMP; ++q) {
-                const double kk = (double)o[q];
-                if (STAGE == 1) {
-                    u[q] = (TOUT)(x0[q] + (0.5 * dt) * kk);
-                    anew[q] = x0[q] + (dt / 6.0) * kk;
-                } else if (STAGE == 2 || STAGE == 3) {
-                    const double y = ys[q * R * TZ];
-                    u[q] = (TOUT)(y + (STAGE == 2 ? 0.5 * dt : dt) * kk);
-                    if (!AD)
-                        anew[q] = as[q * R * TZ] + (dt / 3.0) * kk;
-                    else if (STAGE == 3)
-                        anew[q] = y + (as[q * R * TZ] - y) * (1.0 / 3.0) +
-                                  (x0[q] - y) * (2.0 / 3.0) + (dt / 3.0) * kk;
-                    else
-                        anew[q] = 0.0;  // stage 2 leaves A alone
-                } else {
-                    u[q] = (TOUT)(as[q * R * TZ] + (dt / 6.0) * kk);
+                const double kk = o[q];
+                if constexpr (INC) {
+                    // the base state at this cell: stage 1 reads Y itself
+                    const double y = STAGE == 1 ? c[q] : yrow[q * YW + lane];
+                    if (STAGE <= 3) {
+                        u[q] = (TOUT)((STAGE == 3 ? dt : 0.5 * dt) * kk);
+                        um[q] = y + (double)u[q];
+                    } else {
+                        const double d1 = (double)d1s[q * TZ];
+                        const double d2 = (double)d1s[NCOMP * R * TZ + q * TZ];
+                        const double d3 = (double)xrow[q * XW + lane];
+                        const double yn = y + (d1 + 2.0 * d2 + d3) * (1.0 / 3.0) + (dt / 6.0) * kk;
+                        u[q] = (TOUT)yn;
+                        um[q] = yn;
+                    }
                     anew[q] = 0.0;
+                } else {
+                    if (STAGE == 1) {
+                        u[q] = (TOUT)(c[q] + (0.5 * dt) * kk);
+                        anew[q] = 0.0;
+                    } else if (STAGE == 2 || STAGE == 3) {
+                        const double y = ys[q * TZ];
+                        u[q] = (TOUT)(y + (STAGE == 2 ? 0.5 * dt : dt) * kk);
+                        anew[q] = STAGE == 3 ? y + (as[q * TZ] - y) * (1.0 / 3.0) +
+                                                   (c[q] - y) * (2.0 / 3.0) + (dt / 3.0) * kk
+                                             : 0.0;  // stage 2 leaves A alone
+                    } else {
+                        u[q] = (TOUT)(as[q * TZ] + (dt / 6.0) * kk);
+                        anew[q] = 0.0;
+                    }
+                    um[q] = (double)u[q];
                 }
             }
             // this warp is done with the buffer (after a failed wait it keeps
@@ -534,7 +606,7 @@ __global__ void __launch_bounds__(tma::NTHR, MINB)
                 for (int q = 0; q < NCOMP; ++q) {
                     TOUT *row = U + q * a.cs + ro;
                     row[z] = u[q];
-                    if (STAGE == 3 || (!AD && STAGE <= 2)) a.A[q * a.cs + ro + z] = anew[q];
+                    if (!INC && STAGE == 3) a.A[q * a.cs + ro + z] = anew[q];
                     if (!open_bc) {
                         if (z < a.H) row[z + a.nz] = u[q];
                         if (z >= a.nz - a.H) row[z - a.nz] = u[q];
@@ -553,9 +625,9 @@ __global__ void __launch_bounds__(tma::NTHR, MINB)
                     }
                 }
                 if (coll) {
-                    const double Am = (double)u[EXI] + (double)u[BEXI];
-                    const double Bm = (double)u[EXR] - (double)u[BEXR];
-                    const double Cm = (double)u[EE] - (double)u[XX] - (double)u[BEE] + (double)u[BXX];
+                    const double Am = um[EXI] + um[BEXI];
+                    const double Bm = um[EXR] - um[BEXR];
+                    const double Cm = um[EE] - um[XX] - um[BEE] + um[BXX];
                     macc[0] += Am;
                     macc[1] += Bm;
                     macc[2] += Cm;
@@ -616,15 +688,16 @@ static EncodeTiledFn encode_fn()
     return fn;
 }
 
-// 3-D map over one 8-component buffer: (cells of a padded row, rows, components)
+// 3-D map over one 8-component buffer: (cells of a padded row, components,
+// rows), so that a box lands in shared memory as [row][component][cell]
 int make_state_map(CUtensorMap *map, const void *base, int elem_bytes, int ld, int nvz,
                    long long cs, int box_cells)
 {
     EncodeTiledFn fn = encode_fn();
     if (!fn) return -1;
-    cuuint64_t dims[3] = {(cuuint64_t)ld, (cuuint64_t)nvz, (cuuint64_t)NCOMP};
-    cuuint64_t strides[2] = {(cuuint64_t)ld * elem_bytes, (cuuint64_t)cs * elem_bytes};
-    cuuint32_t box[3] = {(cuuint32_t)box_cells, (cuuint32_t)tma::R, (cuuint32_t)NCOMP};
+    cuuint64_t dims[3] = {(cuuint64_t)ld, (cuuint64_t)NCOMP, (cuuint64_t)nvz};
+    cuuint64_t strides[2] = {(cuuint64_t)cs * elem_bytes, (cuuint64_t)ld * elem_bytes};
+    cuuint32_t box[3] = {(cuuint32_t)box_cells, (cuuint32_t)NCOMP, (cuuint32_t)tma::R};
     cuuint32_t es[3] = {1, 1, 1};
     CUresult r = fn(map, elem_bytes == 8 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64
                                          : CU_TENSOR_MAP_DATA_TYPE_FLOAT32,
@@ -634,7 +707,7 @@ int make_state_map(CUtensorMap *map, const void *base, int elem_bytes, int ld, i
     return r == CUDA_SUCCESS ? 0 : (int)r;
 }
 
-int tma_box_x() { return tma::XW; }
+int tma_box_x(int elem_bytes) { return elem_bytes == 8 ? tma::xw<double>() : tma::xw<float>(); }
 int tma_box_tile() { return tma::TZ; }
 // largest nvz the TMA layout is offered for (the range its tests cover; the
 // kernel itself keeps no per-row state in shared memory)
@@ -644,10 +717,10 @@ static const int TMA_SMEM_MAX = 232448;  // opt-in shared memory per block on sm
 static const int TMA_SMEM_SM = 233472;   // shared memory per SM (1 KB reserved per block)
 
 // Shared memory of one block with an NB-deep ring.
-template <class TIN, int STAGE>
+template <class TIN, class TOUT, int STAGE>
 static int tma_smem(int NB)
 {
-    using L = tma::Layout<TIN, STAGE>;
+    using L = tma::Layout<TIN, TOUT, STAGE>;
     return NB * L::BUF + 2 * NB * 8 + (1 + tma::R / 2) * NMOM * tma::TZ * 8 +
            (int)sizeof(StageArgs);
 }
@@ -657,13 +730,18 @@ static int tma_smem_limit(int minb)
     return minb == 1 ? TMA_SMEM_MAX : TMA_SMEM_SM / minb - 1024;
 }
 
-template <int SCHEME, bool GEN, int STAGE, class TC, class TIN, class TOUT, int NB, int MINB>
-static cudaError_t launch_nb(const CUtensorMap &mX, const CUtensorMap &mY, const CUtensorMap &mA,
-                             const StageArgs &a, int *err, int nblocks, cudaStream_t s,
-                             const BatchDev *bd)
+// The operand maps of one launch: X (stage input with halo), Y, A and B (see
+// Layout; unused ones are ignored).
+struct StageMaps {
+    const CUtensorMap *x, *y, *a, *b;
+};
+
+template <int SCHEME, bool GEN, int STAGE, class TIN, class TOUT, int NB, int MINB>
+static cudaError_t launch_nb(const StageMaps &m, const StageArgs &a, int *err, int nblocks,
+                             cudaStream_t s, const BatchDev *bd)
 {
-    auto kern = rk4_stage_tma_kernel<SCHEME, GEN, STAGE, TC, TIN, TOUT, NB, false, MINB>;
-    auto kernb = rk4_stage_tma_kernel<SCHEME, GEN, STAGE, TC, TIN, TOUT, NB, true, MINB>;
+    auto kern = rk4_stage_tma_kernel<SCHEME, GEN, STAGE, TIN, TOUT, NB, false, MINB>;
+    auto kernb = rk4_stage_tma_kernel<SCHEME, GEN, STAGE, TIN, TOUT, NB, true, MINB>;
     if (nblocks <= 0) {  // preparation call: shared-memory limit and carveout
         for (auto k : {kern, kernb}) {
             cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -675,11 +753,11 @@ static cudaError_t launch_nb(const CUtensorMap &mX, const CUtensorMap &mY, const
         }
         return cudaSuccess;
     }
-    const int shmem = tma_smem<TIN, STAGE>(NB);
+    const int shmem = tma_smem<TIN, TOUT, STAGE>(NB);
     if (bd)
-        kernb<<<nblocks, tma::NTHR, shmem, s>>>(mX, mY, mA, a, err, *bd);
+        kernb<<<nblocks, tma::NTHR, shmem, s>>>(*m.x, *m.y, *m.a, *m.b, a, err, *bd);
     else
-        kern<<<nblocks, tma::NTHR, shmem, s>>>(mX, mY, mA, a, err, BatchDev{});
+        kern<<<nblocks, tma::NTHR, shmem, s>>>(*m.x, *m.y, *m.a, *m.b, a, err, BatchDev{});
     return cudaGetLastError();
 }
 
@@ -687,8 +765,8 @@ static cudaError_t launch_nb(const CUtensorMap &mX, const CUtensorMap &mY, const
 // 4 buffers that total at most ~112 KB.  Measured at nz 32768 x nvz 256, more
 // bytes in flight per SM lower the achieved HBM bandwidth (FP64 stages 2-3,
 // 53 KB per chunk: 0.441 / 0.534 / 0.545 ms per stage with 2 / 3 / 4 buffers;
-// FP64 stage 4, 37 KB: 3 buffers best; FP32 stages 2-3, 43 KB: 2 best; FP64
-// stage 1, 20 KB: 4 buffers 0.318 ms, 5 buffers 0.344 ms).
+// FP64 stage 4, 37 KB: 3 buffers best; FP64 stage 1, 20 KB: 4 buffers
+// 0.318 ms, 5 buffers 0.344 ms).
 // COSENU_TMA_RING=n (2..4) overrides the depth where it fits.
 static int tma_ring_env()
 {
@@ -700,15 +778,15 @@ static int tma_ring_env()
     return v;
 }
 
-template <class TIN, int STAGE>
+template <class TIN, class TOUT, int STAGE>
 static int tma_fd_ring()
 {
-    using L = tma::Layout<TIN, STAGE>;
+    using L = tma::Layout<TIN, TOUT, STAGE>;
     int nb = 2;
     while (nb < 4 && (nb + 1) * L::BUF <= 112 * 1024) ++nb;
     const int e = tma_ring_env();
     if (e) nb = e;
-    while (nb > 2 && tma_smem<TIN, STAGE>(nb) > tma_smem_limit(1)) --nb;
+    while (nb > 2 && tma_smem<TIN, TOUT, STAGE>(nb) > tma_smem_limit(1)) --nb;
     return nb;
 }
 
@@ -728,13 +806,11 @@ static int tma_minb_env()
 
 int tma_blocks_per_sm(int scheme) { return scheme == FV ? tma_minb_env() : 1; }
 
-template <int SCHEME, bool GEN, int STAGE, class TC, class TIN, class TOUT>
-static cudaError_t launch_one(const CUtensorMap &mX, const CUtensorMap &mY, const CUtensorMap &mA,
-                              const StageArgs &a, int *err, int nblocks, cudaStream_t s,
-                              const BatchDev *bd)
+template <int SCHEME, bool GEN, int STAGE, class TIN, class TOUT>
+static cudaError_t launch_one(const StageMaps &m, const StageArgs &a, int *err, int nblocks,
+                              cudaStream_t s, const BatchDev *bd)
 {
-#define LNB(NB, MINB) \
-    launch_nb<SCHEME, GEN, STAGE, TC, TIN, TOUT, NB, MINB>(mX, mY, mA, a, err, nblocks, s, bd)
+#define LNB(NB, MINB) launch_nb<SCHEME, GEN, STAGE, TIN, TOUT, NB, MINB>(m, a, err, nblocks, s, bd)
     if constexpr (SCHEME == FD) {
         if (nblocks <= 0) {
             cudaError_t e = LNB(2, 1);
@@ -742,7 +818,7 @@ static cudaError_t launch_one(const CUtensorMap &mX, const CUtensorMap &mY, cons
             if (e == cudaSuccess) e = LNB(4, 1);
             return e;
         }
-        switch (tma_fd_ring<TIN, STAGE>()) {
+        switch (tma_fd_ring<TIN, TOUT, STAGE>()) {
         case 2: return LNB(2, 1);
         case 3: return LNB(3, 1);
         default: return LNB(4, 1);
@@ -757,47 +833,46 @@ static cudaError_t launch_one(const CUtensorMap &mX, const CUtensorMap &mY, cons
         }
         if (tma_minb_env() == 1) return LNB(4, 1);
         const int lim = tma_smem_limit(2);
-        if (tma_smem<TIN, STAGE>(4) <= lim) return LNB(4, 2);
-        if (tma_smem<TIN, STAGE>(3) <= lim) return LNB(3, 2);
+        if (tma_smem<TIN, TOUT, STAGE>(4) <= lim) return LNB(4, 2);
+        if (tma_smem<TIN, TOUT, STAGE>(3) <= lim) return LNB(3, 2);
         return LNB(2, 2);
     }
 #undef LNB
 }
 
 template <int SCHEME, bool GEN>
-static cudaError_t launch_p(const CUtensorMap &mX, const CUtensorMap &mY, const CUtensorMap &mA,
-                            const StageArgs &a, int stage, int fp32, int *err, int nblocks,
-                            cudaStream_t s, const BatchDev *bd)
+static cudaError_t launch_p(const StageMaps &m, const StageArgs &a, int stage, int fp32, int *err,
+                            int nblocks, cudaStream_t s, const BatchDev *bd)
 {
     if (fp32) {
+        // FP32-bulk: Y in, D1 out; Y + D1 in, D2 out; Y + D2 in, D3 out; Y + D3 in, Y' out
         switch (stage) {
-        // FD stage 1 keeps FP64 arithmetic on its FP64 input (see stage.cu)
-        case 1: return launch_one<SCHEME, GEN, 1, std::conditional_t<SCHEME == FD, double, float>,
-                                  double, float>(mX, mY, mA, a, err, nblocks, s, bd);
-        case 2: return launch_one<SCHEME, GEN, 2, float, float, float>(mX, mY, mA, a, err, nblocks, s, bd);
-        case 3: return launch_one<SCHEME, GEN, 3, float, float, float>(mX, mY, mA, a, err, nblocks, s, bd);
-        case 4: return launch_one<SCHEME, GEN, 4, float, float, double>(mX, mY, mA, a, err, nblocks, s, bd);
+        case 1: return launch_one<SCHEME, GEN, 1, double, float>(m, a, err, nblocks, s, bd);
+        case 2: return launch_one<SCHEME, GEN, 2, float, float>(m, a, err, nblocks, s, bd);
+        case 3: return launch_one<SCHEME, GEN, 3, float, float>(m, a, err, nblocks, s, bd);
+        case 4: return launch_one<SCHEME, GEN, 4, float, double>(m, a, err, nblocks, s, bd);
         }
     } else {
         switch (stage) {
-        case 1: return launch_one<SCHEME, GEN, 1, double, double, double>(mX, mY, mA, a, err, nblocks, s, bd);
-        case 2: return launch_one<SCHEME, GEN, 2, double, double, double>(mX, mY, mA, a, err, nblocks, s, bd);
-        case 3: return launch_one<SCHEME, GEN, 3, double, double, double>(mX, mY, mA, a, err, nblocks, s, bd);
-        case 4: return launch_one<SCHEME, GEN, 4, double, double, double>(mX, mY, mA, a, err, nblocks, s, bd);
+        case 1: return launch_one<SCHEME, GEN, 1, double, double>(m, a, err, nblocks, s, bd);
+        case 2: return launch_one<SCHEME, GEN, 2, double, double>(m, a, err, nblocks, s, bd);
+        case 3: return launch_one<SCHEME, GEN, 3, double, double>(m, a, err, nblocks, s, bd);
+        case 4: return launch_one<SCHEME, GEN, 4, double, double>(m, a, err, nblocks, s, bd);
         }
     }
     return cudaErrorInvalidValue;
 }
 
 cudaError_t launch_rk4_stage_tma(const CUtensorMap &mX, const CUtensorMap &mY,
-                                 const CUtensorMap &mA, const StageArgs &a, int scheme, int stage,
-                                 int fp32, int *err, int nblocks, cudaStream_t s)
+                                 const CUtensorMap &mA, const CUtensorMap &mB, const StageArgs &a,
+                                 int scheme, int stage, int fp32, int *err, int nblocks,
+                                 cudaStream_t s)
 {
-    if (scheme == FV)
-        return launch_p<FV, false>(mX, mY, mA, a, stage, fp32, err, nblocks, s, nullptr);
+    const StageMaps m{&mX, &mY, &mA, &mB};
+    if (scheme == FV) return launch_p<FV, false>(m, a, stage, fp32, err, nblocks, s, nullptr);
     const bool gen = a.fd_advec != 0 || a.ko_order == 5;
-    return gen ? launch_p<FD, true>(mX, mY, mA, a, stage, fp32, err, nblocks, s, nullptr)
-               : launch_p<FD, false>(mX, mY, mA, a, stage, fp32, err, nblocks, s, nullptr);
+    return gen ? launch_p<FD, true>(m, a, stage, fp32, err, nblocks, s, nullptr)
+               : launch_p<FD, false>(m, a, stage, fp32, err, nblocks, s, nullptr);
 }
 
 // Ensemble launch: `a` carries the variant switches shared by every instance
@@ -806,12 +881,12 @@ cudaError_t launch_rk4_stage_tma_batch(const BatchDev &bd, const StageArgs &a, i
                                        int stage, int fp32, int *err, int nblocks, int max_nvz,
                                        cudaStream_t s)
 {
-    CUtensorMap m{};
-    if (scheme == FV)
-        return launch_p<FV, false>(m, m, m, a, stage, fp32, err, nblocks, s, &bd);
+    CUtensorMap z{};
+    const StageMaps m{&z, &z, &z, &z};
+    if (scheme == FV) return launch_p<FV, false>(m, a, stage, fp32, err, nblocks, s, &bd);
     const bool gen = a.fd_advec != 0 || a.ko_order == 5;
-    return gen ? launch_p<FD, true>(m, m, m, a, stage, fp32, err, nblocks, s, &bd)
-               : launch_p<FD, false>(m, m, m, a, stage, fp32, err, nblocks, s, &bd);
+    return gen ? launch_p<FD, true>(m, a, stage, fp32, err, nblocks, s, &bd)
+               : launch_p<FD, false>(m, a, stage, fp32, err, nblocks, s, &bd);
 }
 
 // Sets the shared-memory attribute of every instantiation on the current device.
@@ -825,7 +900,7 @@ cudaError_t tma_prepare()
                 for (int st = 1; st <= 4; ++st) {
                     a.fd_advec = gen;
                     a.ko_order = 3;
-                    cudaError_t e = launch_rk4_stage_tma(m, m, m, a, sch, st, fp32, nullptr, 0,
+                    cudaError_t e = launch_rk4_stage_tma(m, m, m, m, a, sch, st, fp32, nullptr, 0,
                                                          nullptr);
                     if (e != cudaSuccess) return e;
                 }

@@ -48,14 +48,14 @@ __device__ __forceinline__ double weno7_face(double a, double b, double c, doubl
     return d + num / den;
 }
 
-// FP32 variant: indicators and candidates on differences from the centre
-// value as above (which removes the cancellation that FP32 would otherwise
-// suffer on O(1) data), and the weights use fast reciprocals.
-__device__ __forceinline__ float weno7_face(float a, float b, float c, float d, float e, float f,
-                                            float g)
+// FP32-bulk form: the face value minus the centre value from the six
+// stencil differences A..G = u[-3..3] - u[0] (skipping the centre), which the
+// caller takes in FP64 so that FP32 sees only the small differences and not
+// the O(1) values.  Same indicators, candidates and weights as above; the
+// weights use fast reciprocals.
+__device__ __forceinline__ float weno7_corr(float A, float B, float Cc, float E, float F, float G)
 {
     const float eps = 1e-6f;
-    float A = a - d, B = b - d, Cc = c - d, E = e - d, F = f - d, G = g - d;
     float s0 = E * (11003.f * E - 17246.f * F + 4642.f * G) + F * (7043.f * F - 3882.f * G) +
                547.f * G * G;
     float s1 = Cc * (547.f * Cc + 1922.f * E - 494.f * F) + E * (2843.f * E - 1642.f * F) +
@@ -73,7 +73,7 @@ __device__ __forceinline__ float weno7_face(float a, float b, float c, float d, 
     float w2 = __fdividef(12.f, (eps + s2) * (eps + s2));
     float w3 = __fdividef(1.f, (eps + s3) * (eps + s3));
     float num = w0 * q0 + w1 * q1 + w2 * q2 + w3 * q3;
-    return d + __fdividef(num, 12.f * (w0 + w1 + w2 + w3));
+    return __fdividef(num, 12.f * (w0 + w1 + w2 + w3));
 }
 
 }  // namespace cosenu

@@ -54,8 +54,9 @@ enum { COSENU_VAC = 1u, COSENU_MAT = 2u, COSENU_COLL = 4u, COSENU_ADVEC_OFF = 8u
 /* FD advection stencil: ADVEC_CENTER_FD / ADVEC_UPWIND / lopsided
  * (src/rhs_fd.hpp:53-73) */
 enum { COSENU_FD_CENTER = 0, COSENU_FD_UPWIND = 1, COSENU_FD_LOPSIDED = 2 };
-/* arithmetic: plain FP64, or FP32 stage values with FP64 velocity moments,
- * RK4 accumulator and base state */
+/* arithmetic: plain FP64, or FP32-bulk: the RK4 stage increments stored in
+ * FP32 over an FP64 base state, with FP64 velocity moments, accumulation and
+ * diagnostics (FV evaluates its WENO7 weights in FP32 on FP64 differences) */
 enum { COSENU_FP64 = 0, COSENU_FP32_BULK = 1 };
 
 /* Simulation parameters.  Field meanings follow the job.config keys parsed by

@@ -396,77 +396,99 @@ def run_reference_arm(args):
 
 
 def run_ensemble(args):
-    """The ensemble workload: 256 uneven FV instances to t = 1000/mu in one ensemble
-    (autotuned kernel family and tiles), against the plain single-instance
-    FP64 path timed on a stratified subset (every 8th instance, full step
-    counts) and scaled by work."""
+    """The ensemble workload: 256 uneven FV instances to t = 1000/mu.  On N
+    GPUs (torchrun) every rank runs its balanced share as one batched ensemble
+    (autotuned kernel family and tiles) and only the results are gathered;
+    the time is the slowest rank's.  At N = 1 the plain single-instance FP64
+    path is also timed, on a stratified subset (every 8th instance, full step
+    counts) scaled by work, and the batched results are held to it."""
+    import datetime
+
     import torch
 
     from cosenu_b200 import NuOsc
-    from cosenu_b200.ensemble import Ensemble, ensemble_instances
+    from cosenu_b200.distributed import run_ensemble_sharded
+    from cosenu_b200.ensemble import ensemble_instances
 
-    torch.cuda.set_device(0)
-    stream = torch.cuda.Stream()
-    torch.cuda.set_stream(stream)
+    rank, world, local = dist_setup(args.gpus)
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
+                                device_id=torch.device("cuda", local))
     xs = ensemble_instances(args.instances, t_factor=args.t_factor)
     work = [x.cells * x.nsteps for x in xs]
-    ens = Ensemble(xs, precision=args.precision)
-    ens.set_stream(stream.cuda_stream)
-    ens.init_seeded()
-    report = ens.autotune(trial_steps=3)
-    cfg = ens.config()
-    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    with ClockSampler(0) as clk:
-        torch.cuda.synchronize()
-        ev0.record(stream)
-        ens.run()
-        ev1.record(stream)
-        ens.synchronize()
-        torch.cuda.synchronize()
-    t_batch = ev0.elapsed_time(ev1) / 1e3
-    pee = [m.analyse()["Pee"] for m in ens.members]
-    ens.close()
-    # plain path: every 8th instance alone, FP64, default kernel choice
-    sub = list(range(0, len(xs), 8))
-    t_sub = 0.0
-    pee_err = 0.0
-    for i in sub:
-        x = xs[i]
-        sim = NuOsc(nz=x.nz, nvz=x.nvz, gz=4, z0=x.z0, z1=x.z1, cfl=x.cfl, omega=0.0, mu=x.mu,
-                    scheme="fv")
-        sim.set_stream(stream.cuda_stream)
-        sim.init_seeded(x.seed, instance=i, sig_nu=x.sig_nu, sig_nubar=x.sig_nubar,
-                        alpha=x.alpha)
-        torch.cuda.synchronize()
-        ev0.record(stream)
-        sim.evolve(x.nsteps)
-        ev1.record(stream)
-        torch.cuda.synchronize()
-        t_sub += ev0.elapsed_time(ev1) / 1e3
-        if args.precision == "fp64":
-            d = abs(sim.analyse()["Pee"] - pee[i])
-            if d > 1e-9:
-                raise SystemExit(f"ensemble member {i} differs from the plain path: {d}")
-        else:
-            pee_err = max(pee_err, abs(sim.analyse()["Pee"] - pee[i]))
-        sim.close()
-    w_sub = sum(work[i] for i in sub)
-    t_plain = t_sub * sum(work) / w_sub
+    stream = torch.cuda.Stream()
+    torch.cuda.set_stream(stream)
+    cfg = {}
+
+    def runner(chunk, **kw):
+        from cosenu_b200.ensemble import run_on_gpu
+        res, secs, c = run_on_gpu(chunk, **kw)
+        cfg.update(c)
+        return res, secs
+
+    with ClockSampler(local) as clk:
+        results, t_batch, share = run_ensemble_sharded(
+            xs, dist, runner=runner, reduce_device=torch.device("cuda", local),
+            precision=args.precision, device=local, stream=stream)
+    pee = [r["Pee"] for r in results]
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank != 0:
+        return
     n = len(xs)
-    print(json.dumps({
+    line = {
         "metric": "instances/s (256-instance FV ensemble to t = 1000/mu)", "value": n / t_batch,
-        "unit": "instances/s", "n_gpus": 1, "instances": n,
+        "unit": "instances/s", "n_gpus": world, "instances": n,
         "cell_updates_per_s": sum(work) / t_batch, "seconds": t_batch,
-        "plain_fp64_instances_per_s": n / t_plain,
-        "plain_fp64_note": f"{len(sub)} of {n} instances run alone ({t_sub:.1f} s), scaled by work",
-        "speedup_vs_plain": t_plain / t_batch, "higher_is_better": True,
-        "max_abs_err_final_Pee_vs_plain_fp64": pee_err if args.precision != "fp64" else 0.0,
-        "precision": args.precision.upper(), "data": "synthetic",
+        "higher_is_better": True, "scaling": "strong", "precision": args.precision.upper(),
+        "data": "synthetic",
         "config": {"workload": "256 FV WENO7 instances, nz logU[512,8192]/256, nvz {32..256}, "
                                "alpha U[.6,1.2], sigma U[.4,.8]/U[.3,.7], mu U[.5,2], "
-                               "t = 1000/mu", "kernel": cfg, "t_factor": args.t_factor},
-        "autotune": report.strip().splitlines(), "clocks": clk.summary(),
-    }), flush=True)
+                               "t = 1000/mu", "t_factor": args.t_factor,
+                   "sharding": f"{world} ranks, members partitioned by nz*nvz*steps, results "
+                               "gathered, time max over ranks",
+                   "kernel (rank 0)": {k: v for k, v in cfg.items() if k != "autotune"},
+                   "rank0_members": len(share)},
+        "autotune (rank 0)": cfg.get("autotune", []), "clocks": clk.summary(),
+    }
+    if world == 1:
+        # plain path: every 8th instance alone, FP64, default kernel choice
+        sub = list(range(0, n, 8))
+        t_sub = 0.0
+        pee_err = 0.0
+        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        for i in sub:
+            x = xs[i]
+            sim = NuOsc(nz=x.nz, nvz=x.nvz, gz=4, z0=x.z0, z1=x.z1, cfl=x.cfl, omega=0.0,
+                        mu=x.mu, scheme="fv")
+            sim.set_stream(stream.cuda_stream)
+            sim.init_seeded(x.seed, instance=x.index, sig_nu=x.sig_nu, sig_nubar=x.sig_nubar,
+                            alpha=x.alpha)
+            torch.cuda.synchronize()
+            ev0.record(stream)
+            sim.evolve(x.nsteps)
+            ev1.record(stream)
+            torch.cuda.synchronize()
+            t_sub += ev0.elapsed_time(ev1) / 1e3
+            d = abs(sim.analyse()["Pee"] - pee[i])
+            if args.precision == "fp64" and d > 1e-9:
+                raise SystemExit(f"ensemble member {i} differs from the plain path: {d}")
+            pee_err = max(pee_err, d)
+            sim.close()
+        w_sub = sum(work[i] for i in sub)
+        t_plain = t_sub * sum(work) / w_sub
+        line.update({
+            "plain_fp64_instances_per_s": n / t_plain,
+            "plain_fp64_note": f"{len(sub)} of {n} instances run alone ({t_sub:.1f} s), "
+                               "scaled by work",
+            "speedup_vs_plain": t_plain / t_batch,
+            "max_abs_err_final_Pee_vs_plain_fp64": pee_err,
+            "err_subset": f"the {len(sub)} instances run alone"})
+    print(json.dumps(line), flush=True)
 
 
 def run_fp32_study(args):

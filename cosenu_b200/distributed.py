@@ -63,3 +63,32 @@ def max_over_ranks(value: float, dist=None, device=None) -> float:
     t = torch.tensor([value], dtype=torch.float64, device=device)
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
+
+
+def run_ensemble_sharded(instances: Sequence, dist=None, runner: Callable | None = None,
+                         reduce_device=None, **runner_kw):
+    """The ensemble workload over all ranks: this rank's share of `instances`
+    (balanced by nz * nvz * steps, partition_work) runs as one batched
+    ensemble (`runner`, default ensemble.run_on_gpu); every member's result
+    comes back to every rank in instance order and the run time is the
+    slowest rank's.  Returns (results, seconds, this rank's share).  The
+    reference's counterpart is one process per configuration
+    (manage.py:361-428); here the only exchange is the final gather."""
+    if runner is None:
+        from .ensemble import run_on_gpu as runner
+    weights = [x.cells * x.nsteps for x in instances]
+    world = dist.get_world_size() if dist is not None and dist.is_initialized() else 1
+    rank = dist.get_rank() if world > 1 else 0
+    share = partition_work(weights, world)[rank]
+    timing = {"seconds": 0.0}
+
+    def work(chunk):
+        if not chunk:
+            return []
+        res, secs = runner(list(chunk), **runner_kw)[:2]
+        timing["seconds"] = secs
+        return res
+
+    results = run_sharded(instances, weights, work, dist)
+    seconds = max_over_ranks(timing["seconds"], dist, reduce_device)
+    return results, seconds, share

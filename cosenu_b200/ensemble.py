@@ -32,6 +32,10 @@ class Instance:
     z0: float = -600.0
     z1: float = 600.0
     cfl: float = 0.4
+    # position in the whole workload: keys the member's random perturbation, so
+    # that it does not depend on which ensemble (or rank) runs the member;
+    # -1: its position in the ensemble that runs it
+    index: int = -1
 
     @property
     def cells(self) -> int:
@@ -68,7 +72,7 @@ def ensemble_instances(n: int = 256, seed: int = 20240601, t_factor: float = 100
         sig_nubar = float(rng.uniform(0.3, 0.7))
         mu = float(rng.uniform(0.5, 2.0))
         out.append(Instance(nz, nvz, alpha, sig_nu, sig_nubar, mu, seed=seed * 1000 + i,
-                            nsteps=steps_to(t_factor / mu, nz)))
+                            nsteps=steps_to(t_factor / mu, nz), index=i))
     return out
 
 
@@ -114,6 +118,13 @@ class Ensemble:
         return len(self.instances)
 
     def init_seeded(self, amp: float = 1e-6) -> None:
+        """Seeded initial conditions (cosenu_init_seeded per member); a member's
+        perturbation is keyed by its seed and its index in the workload."""
+        if all(x.index >= 0 for x in self.instances):
+            for m, x in zip(self.members, self.instances):
+                m.init_seeded(x.seed, instance=x.index, sig_nu=x.sig_nu, sig_nubar=x.sig_nubar,
+                              alpha=x.alpha, amp=amp)
+            return
         n = len(self)
         seeds = (C.c_uint64 * n)(*[x.seed for x in self.instances])
         d = lambda key: (C.c_double * n)(*[getattr(x, key) for x in self.instances])  # noqa: E731
@@ -147,3 +158,33 @@ class Ensemble:
         n = len(self)
         arr = (C.c_int * n)(*(tv if tv is not None else [min(64, x.nvz) for x in self.instances]))
         self._check(self.lib.cosenu_batch_set_config(self.h, int(use_tma), tz, arr))
+
+
+def run_on_gpu(instances: list[Instance], precision: str = "fp64", device: int = 0,
+               trial_steps: int = 3, stream=None) -> tuple[list[dict], float, dict]:
+    """Runs `instances` as one batched ensemble on one GPU: seeded initial
+    conditions, autotuned kernel family and tiles, every member to its own
+    step count.  Returns the per-member end-of-run analysis (the keys of
+    NuOsc.analyse), the device time of the run in seconds (CUDA events on the
+    ensemble's stream) and the chosen kernel configuration."""
+    import torch
+    torch.cuda.set_device(device)
+    if stream is None:
+        stream = torch.cuda.Stream(device=device)
+    with Ensemble(instances, precision=precision, device=device) as ens:
+        ens.set_stream(stream.cuda_stream)
+        ens.init_seeded()
+        report = ens.autotune(trial_steps=trial_steps) if trial_steps > 0 else ""
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize(device)
+        e0.record(stream)
+        ens.run()
+        e1.record(stream)
+        ens.synchronize()
+        torch.cuda.synchronize(device)
+        seconds = e0.elapsed_time(e1) / 1e3
+        results = [m.analyse() for m in ens.members]
+        cfg = ens.config()
+        cfg["autotune"] = report.strip().splitlines()
+    return results, seconds, cfg

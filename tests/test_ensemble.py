@@ -133,3 +133,27 @@ def test_ensemble_fp32_bulk_close_to_fp64(gpu_lib):
             outs.append([m.download() for m in ens.members])
     for a, b in zip(*outs):
         assert np.abs(a - b).max() <= 1e-5
+
+
+@pytest.mark.gpu
+def test_sharded_runner_on_one_gpu_matches_members_run_alone(gpu_lib):
+    """run_ensemble_sharded on one process (the path bench.py's ensemble
+    workload takes at every N): autotuned ensemble, every member's final
+    analysis equal to the member run alone to 1e-12."""
+    import dataclasses
+
+    from cosenu_b200 import NuOsc
+    from cosenu_b200.distributed import run_ensemble_sharded
+    xs = [dataclasses.replace(x, index=i) for i, x in enumerate(_small())]
+    res, secs, share = run_ensemble_sharded(xs, None, trial_steps=1)
+    assert share == list(range(len(xs))) and secs > 0
+    for i, x in enumerate(xs):
+        sim = NuOsc(nz=x.nz, nvz=x.nvz, gz=4, z0=x.z0, z1=x.z1, cfl=x.cfl, omega=0.0, mu=x.mu,
+                    scheme="fv")
+        sim.init_seeded(x.seed, instance=i, sig_nu=x.sig_nu, sig_nubar=x.sig_nubar,
+                        alpha=x.alpha)
+        sim.evolve(x.nsteps)
+        a = sim.analyse()
+        sim.close()
+        for k in ("Pee", "Pbee", "M0", "trace", "eln"):
+            assert abs(a[k] - res[i][k]) <= 1e-12 * max(1.0, abs(a[k])), (i, k)

@@ -582,6 +582,16 @@ def run_surrogate(args):
     t0 = time.perf_counter()
     losses = sur.fit(x_train, y_train, epochs=args.epochs, batch=64, lr=2e-3)
     t_fit = time.perf_counter() - t0
+    # device time per kernel class: one more training epoch of the committee
+    # and one committee inference over the held-out set, with CUDA events
+    sur.set_timing(True)
+    for k, m in enumerate(sur.models):
+        m.train(epochs=1, batch=64, lr=1e-5, seed=9000 + k)
+    train_ms = sur.timing()
+    sur.set_timing(True)
+    sur.committee(x_test)
+    infer_ms = sur.timing()
+    sur.set_timing(False)
     sur.committee(x_test)  # warm-up at the timed batch size (activation buffers sized)
     t0 = time.perf_counter()
     mean, spread = sur.committee(x_test)
@@ -592,6 +602,30 @@ def run_surrogate(args):
     final[fb] = y_test[fb]  # the solver's own answer where the committee falls back
     t_with_fb = t_net + t_solver * fb.mean()
     err_fb = np.abs(final - y_test)
+    # generalisation beyond the training resolution: held-out instances with
+    # nz log-uniform in [512, 8192] (the ensemble workload's distribution), solver
+    # targets at their own nz
+    gen = {}
+    if args.gen_test > 0:
+        gtest = surrogate_instances(args.gen_test, seed=23, nz=None, t_factor=args.t_factor)
+        t0 = time.perf_counter()
+        y_gen = solve_pee(gtest)
+        t_gen_solver = time.perf_counter() - t0
+        x_gen = np.stack([features(i) for i in gtest])
+        g_mean, g_spread = sur.committee(x_gen)
+        g_err = np.abs(g_mean - y_gen)
+        g_fb = g_spread > args.threshold
+        g_final = g_mean.copy()
+        g_final[g_fb] = y_gen[g_fb]
+        nzs = np.array([i.nz for i in gtest])
+        gen = {"instances": len(gtest), "nz_range": [int(nzs.min()), int(nzs.max())],
+               "mean_abs_err": float(g_err.mean()),
+               "mean_abs_err_nz_le_1024": float(g_err[nzs <= 1024].mean()) if (nzs <= 1024).any() else None,
+               "mean_abs_err_nz_gt_2048": float(g_err[nzs > 2048].mean()) if (nzs > 2048).any() else None,
+               "fallback_fraction": float(g_fb.mean()),
+               "mean_abs_err_with_fallback": float(np.abs(g_final - y_gen).mean()),
+               "solver_seconds": t_gen_solver}
+    tot = lambda d: sum(d.values())  # noqa: E731
     print(json.dumps({
         "metric": "surrogate vs solver on held-out instances", "train": len(train),
         "test": len(test), "nz": args.sur_nz, "nvz": 128, "t_factor": args.t_factor,
@@ -607,6 +641,12 @@ def run_surrogate(args):
         "speedup_with_fallback": t_solver / t_with_fb,
         "train_data_seconds": t_train_data, "train_seconds": t_fit,
         "final_train_loss": [float(ls[-1]) for ls in losses],
+        "device_ms_per_kernel_class": {
+            "training_one_epoch_committee": train_ms,
+            "training_gemm_share": train_ms["gemm"] / tot(train_ms),
+            "inference_committee": infer_ms,
+            "inference_gemm_share": infer_ms["gemm"] / tot(infer_ms)},
+        "held_out_nz_loguniform": gen,
     }), flush=True)
     sur.close()
 
@@ -689,6 +729,8 @@ def main():
     ap.add_argument("--sur-nz", type=int, default=512, help="c5: nz of the solver runs")
     ap.add_argument("--epochs", type=int, default=300, help="c5: training epochs")
     ap.add_argument("--threshold", type=float, default=1e-2, help="c5: fallback threshold")
+    ap.add_argument("--gen-test", type=int, default=64,
+                    help="c5: held-out instances with nz log-uniform in [512, 8192]")
     ap.add_argument("--fp32-study", action="store_true",
                     help="FP32-bulk vs FP64 error study on the chosen workload")
     ap.add_argument("--study-steps", type=int, default=8000)

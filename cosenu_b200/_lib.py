@@ -36,6 +36,7 @@ EXPORTS = (
     "cosenu_mlp_create", "cosenu_mlp_destroy", "cosenu_mlp_last_error", "cosenu_mlp_num_params",
     "cosenu_mlp_get_params", "cosenu_mlp_set_params", "cosenu_mlp_forward",
     "cosenu_mlp_loss_grad", "cosenu_mlp_set_data", "cosenu_mlp_train",
+    "cosenu_mlp_set_timing", "cosenu_mlp_timing",
 )
 
 
@@ -135,6 +136,8 @@ def load(path: str | None = None) -> C.CDLL:
         "cosenu_mlp_set_data": (i, [vp, vp, vp, i]),
         "cosenu_mlp_train": (i, [vp, i, i, C.c_float, C.c_float, C.c_float, C.c_float,
                                  C.c_float, C.c_uint64, vp]),
+        "cosenu_mlp_set_timing": (i, [vp, i]),
+        "cosenu_mlp_timing": (i, [vp, C.POINTER(d)]),
     }
     for name, (res, args) in sig.items():
         f = getattr(lib, name)

@@ -247,10 +247,68 @@ struct cosenu_mlp {
     int ndata = 0;
     long long t_step = 0;
     cudaStream_t stream = nullptr;
+    // host inputs of forward / loss_grad staged here (grown on demand)
+    float *dxin = nullptr, *dtin = nullptr;
+    size_t xin_cap = 0, tin_cap = 0;
+    // timing mode: CUDA events around every launch, by kernel class
+    bool timing = false;
+    std::vector<std::pair<int, std::pair<cudaEvent_t, cudaEvent_t>>> ev;  // (class, (start, stop))
+    std::vector<cudaEvent_t> ev_pool;
+    double ms[3] = {0, 0, 0};  // GEMM, elementwise, AdamW
     std::string err;
 };
 
 namespace {
+
+enum { K_GEMM = 0, K_ELEM = 1, K_ADAMW = 2 };
+
+cudaEvent_t pool_event(cosenu_mlp *net)
+{
+    if (!net->ev_pool.empty()) {
+        cudaEvent_t e = net->ev_pool.back();
+        net->ev_pool.pop_back();
+        return e;
+    }
+    cudaEvent_t e = nullptr;
+    cudaEventCreate(&e);
+    return e;
+}
+
+// Brackets one launch with events when timing is on: tstart before the
+// launch, tstop after it.
+struct Timed {
+    cosenu_mlp *net;
+    int cls;
+    cudaEvent_t a = nullptr;
+    Timed(cosenu_mlp *n, int c) : net(n), cls(c)
+    {
+        if (net->timing) {
+            a = pool_event(net);
+            cudaEventRecord(a, net->stream);
+        }
+    }
+    ~Timed()
+    {
+        if (net->timing) {
+            cudaEvent_t b = pool_event(net);
+            cudaEventRecord(b, net->stream);
+            net->ev.push_back({cls, {a, b}});
+        }
+    }
+};
+
+// After a synchronisation: adds the recorded intervals to the class totals.
+void collect_times(cosenu_mlp *net)
+{
+    for (auto &e : net->ev) {
+        float t = 0.f;
+        if (cudaEventElapsedTime(&t, e.second.first, e.second.second) == cudaSuccess)
+            net->ms[e.first] += t;
+        net->ev_pool.push_back(e.second.first);
+        net->ev_pool.push_back(e.second.second);
+    }
+    net->ev.clear();
+}
 
 int mfail(cosenu_mlp *n, int code, const std::string &msg)
 {
@@ -264,6 +322,30 @@ int mfail(cosenu_mlp *n, int code, const std::string &msg)
         if (e_ != cudaSuccess)                                                                \
             return mfail(net, COSENU_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); \
     } while (0)
+
+// Host rows (and targets) copied into the staging buffers, grown on demand.
+int stage_inputs(cosenu_mlp *net, const float *x_host, const float *t_host, int rows)
+{
+    const size_t nx = (size_t)rows * net->nin, nt = (size_t)rows * net->nout;
+    if (nx > net->xin_cap) {
+        cudaStreamSynchronize(net->stream);
+        if (net->dxin) cudaFree(net->dxin);
+        net->dxin = nullptr;
+        MCK(cudaMalloc(&net->dxin, nx * 4));
+        net->xin_cap = nx;
+    }
+    if (t_host && nt > net->tin_cap) {
+        cudaStreamSynchronize(net->stream);
+        if (net->dtin) cudaFree(net->dtin);
+        net->dtin = nullptr;
+        MCK(cudaMalloc(&net->dtin, nt * 4));
+        net->tin_cap = nt;
+    }
+    MCK(cudaMemcpyAsync(net->dxin, x_host, nx * 4, cudaMemcpyHostToDevice, net->stream));
+    if (t_host)
+        MCK(cudaMemcpyAsync(net->dtin, t_host, nt * 4, cudaMemcpyHostToDevice, net->stream));
+    return COSENU_OK;
+}
 
 int ensure_cap(cosenu_mlp *net, int rows)
 {
@@ -296,6 +378,7 @@ void forward(cosenu_mlp *net, int rows)
     int kin = net->kpad;
     for (int l = 0; l < net->nl; ++l) {
         const bool last = l == net->nl - 1;
+        Timed tm(net, K_GEMM);
         gemm(x, kin, 1, net->wb + net->woff[l], 1, kin, rows, net->dout[l], kin, net->Z[l],
              net->dout[l], net->w + net->boff[l], last ? nullptr : net->Hb[l], net->dout[l],
              last ? 0 : 1, net->stream);
@@ -309,23 +392,36 @@ void backward(cosenu_mlp *net, int rows, int nblk_loss)
 {
     const int L = net->nl;
     const int nout = net->nout;
-    mse_kernel<<<nblk_loss, 256, 0, net->stream>>>(net->Z[L - 1], net->T, rows * nout,
-                                                   1.f / ((float)rows * nout), net->dA, net->dAb,
-                                                   net->partial);
+    {
+        Timed tm(net, K_ELEM);
+        mse_kernel<<<nblk_loss, 256, 0, net->stream>>>(net->Z[L - 1], net->T, rows * nout,
+                                                       1.f / ((float)rows * nout), net->dA,
+                                                       net->dAb, net->partial);
+    }
     // dA (FP32) / dAb (BF16) hold dZ of layer l
     for (int l = L - 1; l >= 0; --l) {
         const int din = net->din[l], dout = net->dout[l];
         const __nv_bfloat16 *xin = l == 0 ? net->xb : net->Hb[l - 1];
         // dW[n][k] = sum_m dZ[m][n] X[m][k]
-        gemm(net->dAb, 1, dout, xin, din, 1, dout, din, rows, net->g + net->woff[l], din, nullptr,
-             nullptr, 0, 0, net->stream);
-        colsum_kernel<<<(dout + 127) / 128, 128, 0, net->stream>>>(net->dA, rows, dout,
-                                                                   net->g + net->boff[l]);
+        {
+            Timed tm(net, K_GEMM);
+            gemm(net->dAb, 1, dout, xin, din, 1, dout, din, rows, net->g + net->woff[l], din,
+                 nullptr, nullptr, 0, 0, net->stream);
+        }
+        {
+            Timed tm(net, K_ELEM);
+            colsum_kernel<<<(dout + 127) / 128, 128, 0, net->stream>>>(net->dA, rows, dout,
+                                                                       net->g + net->boff[l]);
+        }
         if (l > 0) {
             // dH[m][k] = sum_n dZ[m][n] W[n][k]; then dZ_{l-1} = dH * gelu'(Z_{l-1})
-            gemm(net->dAb, dout, 1, net->wb + net->woff[l], din, 1, rows, din, dout, net->dB, din,
-                 nullptr, nullptr, 0, 0, net->stream);
+            {
+                Timed tm(net, K_GEMM);
+                gemm(net->dAb, dout, 1, net->wb + net->woff[l], din, 1, rows, din, dout, net->dB,
+                     din, nullptr, nullptr, 0, 0, net->stream);
+            }
             int n = rows * din;
+            Timed tm(net, K_ELEM);
             gelu_back_kernel<<<(n + 255) / 256, 256, 0, net->stream>>>(net->dB, net->Z[l - 1], n,
                                                                        net->dA, net->dAb);
         }
@@ -398,13 +494,15 @@ int cosenu_mlp_destroy(cosenu_mlp *net)
     if (!net) return COSENU_OK;
     if (net->stream) cudaStreamSynchronize(net->stream);
     void *bufs[] = {net->w, net->g, net->m1, net->m2, net->wb, net->partial, net->xb, net->dA,
-                    net->dB, net->dAb, net->T, net->dX, net->dT, net->didx};
+                    net->dB, net->dAb, net->T, net->dX, net->dT, net->didx, net->dxin, net->dtin};
     for (void *b : bufs)
         if (b) cudaFree(b);
     for (auto p : net->Z)
         if (p) cudaFree(p);
     for (auto p : net->Hb)
         if (p) cudaFree(p);
+    collect_times(net);
+    for (cudaEvent_t e : net->ev_pool) cudaEventDestroy(e);
     if (net->stream) cudaStreamDestroy(net->stream);
     delete net;
     return COSENU_OK;
@@ -448,16 +546,17 @@ int cosenu_mlp_forward(cosenu_mlp *net, const float *x_host, int rows, float *y_
     cudaSetDevice(net->device);
     int rc = ensure_cap(net, rows);
     if (rc) return rc;
-    float *dx = nullptr;
-    MCK(cudaMalloc(&dx, (size_t)rows * net->nin * 4));
-    MCK(cudaMemcpyAsync(dx, x_host, (size_t)rows * net->nin * 4, cudaMemcpyHostToDevice, net->stream));
-    gather_kernel<<<rows, 128, 0, net->stream>>>(dx, nullptr, nullptr, rows, net->nin, net->kpad,
-                                                 net->nout, net->xb, nullptr);
+    if ((rc = stage_inputs(net, x_host, nullptr, rows)) != COSENU_OK) return rc;
+    {
+        Timed tm(net, K_ELEM);
+        gather_kernel<<<rows, 128, 0, net->stream>>>(net->dxin, nullptr, nullptr, rows, net->nin,
+                                                     net->kpad, net->nout, net->xb, nullptr);
+    }
     forward(net, rows);
     MCK(cudaMemcpyAsync(y_host, net->Z[net->nl - 1], (size_t)rows * net->nout * 4,
                         cudaMemcpyDeviceToHost, net->stream));
     MCK(cudaStreamSynchronize(net->stream));
-    cudaFree(dx);
+    collect_times(net);
     return COSENU_OK;
 }
 
@@ -470,13 +569,9 @@ int cosenu_mlp_loss_grad(cosenu_mlp *net, const float *x_host, const float *t_ho
     cudaSetDevice(net->device);
     int rc = ensure_cap(net, rows);
     if (rc) return rc;
-    float *dx = nullptr, *dt = nullptr;
-    MCK(cudaMalloc(&dx, (size_t)rows * net->nin * 4));
-    MCK(cudaMalloc(&dt, (size_t)rows * net->nout * 4));
-    MCK(cudaMemcpyAsync(dx, x_host, (size_t)rows * net->nin * 4, cudaMemcpyHostToDevice, net->stream));
-    MCK(cudaMemcpyAsync(dt, t_host, (size_t)rows * net->nout * 4, cudaMemcpyHostToDevice, net->stream));
-    gather_kernel<<<rows, 128, 0, net->stream>>>(dx, dt, nullptr, rows, net->nin, net->kpad,
-                                                 net->nout, net->xb, net->T);
+    if ((rc = stage_inputs(net, x_host, t_host, rows)) != COSENU_OK) return rc;
+    gather_kernel<<<rows, 128, 0, net->stream>>>(net->dxin, net->dtin, nullptr, rows, net->nin,
+                                                 net->kpad, net->nout, net->xb, net->T);
     forward(net, rows);
     const int nb = 64;
     backward(net, rows, nb);
@@ -485,8 +580,7 @@ int cosenu_mlp_loss_grad(cosenu_mlp *net, const float *x_host, const float *t_ho
     if (grad_host)
         MCK(cudaMemcpyAsync(grad_host, net->g, net->nparam * 4, cudaMemcpyDeviceToHost, net->stream));
     MCK(cudaStreamSynchronize(net->stream));
-    cudaFree(dx);
-    cudaFree(dt);
+    collect_times(net);
     double s = 0;
     for (float p : part) s += p;
     if (loss) *loss = (float)(s / ((double)rows * net->nout));
@@ -539,14 +633,18 @@ int cosenu_mlp_train(cosenu_mlp *net, int epochs, int batch, float lr, float wei
         long long ecount = 0;
         for (int b0 = 0; b0 < net->ndata; b0 += batch) {
             const int rows = std::min(batch, net->ndata - b0);
-            gather_kernel<<<rows, 128, 0, net->stream>>>(net->dX, net->dT, net->didx + b0, rows,
-                                                         net->nin, net->kpad, net->nout, net->xb,
-                                                         net->T);
+            {
+                Timed tm(net, K_ELEM);
+                gather_kernel<<<rows, 128, 0, net->stream>>>(net->dX, net->dT, net->didx + b0,
+                                                             rows, net->nin, net->kpad, net->nout,
+                                                             net->xb, net->T);
+            }
             forward(net, rows);
             backward(net, rows, nb);
             net->t_step++;
             const float c1 = 1.f - std::pow(beta1, (float)net->t_step);
             const float c2 = 1.f - std::pow(beta2, (float)net->t_step);
+            Timed *tm = new Timed(net, K_ADAMW);
             for (int l = 0; l < net->nl; ++l) {
                 const long long nw = (long long)net->din[l] * net->dout[l];
                 adamw_kernel<<<(unsigned)((nw + 255) / 256), 256, 0, net->stream>>>(
@@ -558,15 +656,35 @@ int cosenu_mlp_train(cosenu_mlp *net, int epochs, int batch, float lr, float wei
                     net->m2 + net->boff[l], net->wb + net->boff[l], net->dout[l], lr, beta1, beta2,
                     eps, 0.f, c1, c2);
             }
+            delete tm;  // the AdamW updates of all layers
             loss_accumulate_kernel<<<1, 32, 0, net->stream>>>(net->partial, nb, net->eacc);
             ecount += (long long)rows * net->nout;
         }
         // one host synchronisation per epoch (the shuffle buffer is reused)
         MCK(cudaMemcpyAsync(&esum, net->eacc, sizeof(double), cudaMemcpyDeviceToHost, net->stream));
         MCK(cudaStreamSynchronize(net->stream));
+        collect_times(net);
         if (epoch_loss) epoch_loss[e] = (float)(esum / ecount);
     }
     MCK(cudaGetLastError());
+    return COSENU_OK;
+}
+
+int cosenu_mlp_set_timing(cosenu_mlp *net, int on)
+{
+    if (!net) return COSENU_ERR_ARG;
+    cudaSetDevice(net->device);
+    MCK(cudaStreamSynchronize(net->stream));
+    collect_times(net);
+    net->timing = on != 0;
+    net->ms[0] = net->ms[1] = net->ms[2] = 0.0;
+    return COSENU_OK;
+}
+
+int cosenu_mlp_timing(const cosenu_mlp *net, double ms[3])
+{
+    if (!net || !ms) return COSENU_ERR_ARG;
+    for (int k = 0; k < 3; ++k) ms[k] = net->ms[k];
     return COSENU_OK;
 }
 

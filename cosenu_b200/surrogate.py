@@ -45,19 +45,26 @@ def reseeded(instances: list[Instance], offset: int = 7919) -> list[Instance]:
     return [dataclasses.replace(x, seed=x.seed + offset) for x in instances]
 
 
-def surrogate_instances(n: int, seed: int, nz: int = 512, nvz: int = 128,
-                        t_factor: float = 1000.0) -> list[Instance]:
+def surrogate_instances(n: int, seed: int, nz: int | None = 512, nvz: int = 128,
+                        t_factor: float = 1000.0, nz_range=(512, 8192)) -> list[Instance]:
     """Surrogate inputs: the ensemble parameter distribution
-    (ensemble.ensemble_instances) at fixed nvz (and, to keep the training
-    set affordable, fixed nz)."""
+    (ensemble.ensemble_instances) at fixed nvz, with nz fixed (to keep a
+    training set affordable) or, with nz=None, log-uniform in nz_range rounded
+    to 256 as in the ensemble workload."""
     rng = np.random.default_rng(seed)
     out = []
     for i in range(n):
         mu = float(rng.uniform(0.5, 2.0))
-        out.append(Instance(nz=nz, nvz=nvz, alpha=float(rng.uniform(0.6, 1.2)),
+        if nz is None:
+            lo, hi = math.log(nz_range[0]), math.log(nz_range[1])
+            nzi = int(256 * round(math.exp(rng.uniform(lo, hi)) / 256))
+            nzi = min(max(nzi, 256), nz_range[1])
+        else:
+            nzi = nz
+        out.append(Instance(nz=nzi, nvz=nvz, alpha=float(rng.uniform(0.6, 1.2)),
                             sig_nu=float(rng.uniform(0.4, 0.8)),
                             sig_nubar=float(rng.uniform(0.3, 0.7)), mu=mu,
-                            seed=seed * 100000 + i, nsteps=steps_to(t_factor / mu, nz)))
+                            seed=seed * 100000 + i, nsteps=steps_to(t_factor / mu, nzi)))
     return out
 
 
@@ -166,6 +173,16 @@ class MLP:
         self.set_data(x, t)
         return self.train(epochs, batch, lr, weight_decay, seed)
 
+    def set_timing(self, on: bool) -> None:
+        """CUDA-event timing of every later launch by kernel class (clears the totals)."""
+        self._check(self.lib.cosenu_mlp_set_timing(self.h, int(on)))
+
+    def timing(self) -> dict:
+        """Device milliseconds per kernel class since set_timing(True)."""
+        ms = (C.c_double * 3)()
+        self._check(self.lib.cosenu_mlp_timing(self.h, ms))
+        return {"gemm": ms[0], "elementwise": ms[1], "adamw": ms[2]}
+
 
 @dataclass
 class Prediction:
@@ -228,6 +245,18 @@ class Surrogate:
             idx = np.nonzero(fb)[0]
             pee[idx] = solver([instances[i] for i in idx])
         return Prediction(pee=pee, spread=spread, fallback=fb)
+
+    def set_timing(self, on: bool) -> None:
+        for m in self.models:
+            m.set_timing(on)
+
+    def timing(self) -> dict:
+        """Device milliseconds per kernel class, summed over the committee."""
+        out = {"gemm": 0.0, "elementwise": 0.0, "adamw": 0.0}
+        for m in self.models:
+            for k, v in m.timing().items():
+                out[k] += v
+        return out
 
     def close(self):
         for m in self.models:

@@ -281,6 +281,13 @@ int cosenu_mlp_loss_grad(cosenu_mlp *net, const float *x_host, const float *t_ho
 int cosenu_mlp_set_data(cosenu_mlp *net, const float *x_host, const float *t_host, int n);
 int cosenu_mlp_train(cosenu_mlp *net, int epochs, int batch, float lr, float weight_decay,
                      float beta1, float beta2, float eps, uint64_t shuffle_seed, float *epoch_loss);
+/* Timing mode: with on != 0 every later launch is bracketed by CUDA events and
+ * its device time added to one of three classes, read by cosenu_mlp_timing as
+ * ms[0] GEMMs (forward, dX, dW), ms[1] elementwise kernels (gather, MSE,
+ * GELU backward, bias column sums), ms[2] AdamW updates.  Setting the mode
+ * clears the totals. */
+int cosenu_mlp_set_timing(cosenu_mlp *net, int on);
+int cosenu_mlp_timing(const cosenu_mlp *net, double ms[3]);
 
 /* For callers that must not allocate device memory (a host application whose
  * device memory all comes from its own pool, or a loop that cannot afford the

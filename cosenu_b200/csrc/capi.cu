@@ -487,7 +487,9 @@ int ctx_create(const cosenu_params *pp, cosenu_ctx **out, int layout)
         int r = make_state_map(&ctx->mYb40[0], ctx->Yb[0], 8, ctx->ld, p.nvz, ctx->cs, bx);
         if (!r) r = make_state_map(&ctx->mYb40[1], ctx->Yb[1], 8, ctx->ld, p.nvz, ctx->cs, bx);
         if (!r) r = make_state_map(&ctx->mU0_40, ctx->U0, ub, ctx->ld, p.nvz, ctx->cs, bxu);
-        if (!r) r = make_state_map(&ctx->mU1_40, ctx->U1, ub, ctx->ld, p.nvz, ctx->cs, bxu);
+        // (FP64 stage 3 reads U1 in 40-cell rows, see the TMA kernel's Layout)
+        if (!r) r = make_state_map(&ctx->mU1_40, ctx->U1, ub, ctx->ld, p.nvz, ctx->cs,
+                                   ctx->fp32 ? bxu : bt + 8);
         if (!r) r = make_state_map(&ctx->mY32, ctx->Yb[0], 8, ctx->ld, p.nvz, ctx->cs, bt);
         if (!r) r = make_state_map(&ctx->mA32, ctx->Yb[1], 8, ctx->ld, p.nvz, ctx->cs, bt);
         if (!r) r = make_state_map(&ctx->mU0_32, ctx->U0, ub, ctx->ld, p.nvz, ctx->cs, bt);

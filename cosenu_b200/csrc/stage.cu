@@ -61,15 +61,29 @@ template <bool INC, bool YPLUS, class TIN>
 __device__ __forceinline__ double face_at(const TIN *__restrict__ X, const double *__restrict__ Y,
                                           long long i, int dir)
 {
-    double u[7];
+    if constexpr (INC) {
+        // stencil differences as (Y difference in FP64, rounded) + (D
+        // difference in FP32); the face is Y + (D + correction)
+        float d[7];
+        const double y0 = YPLUS ? ld_nc(Y + i) : (double)ld_nc(X + i);
+        const float x0 = YPLUS ? (float)ld_nc(X + i) : 0.f;
 #pragma unroll
-    for (int k = -3; k <= 3; ++k) u[k + 3] = in_at<YPLUS>(X, Y, i + k * dir);
-    if constexpr (INC)
-        return u[3] + (double)weno7_corr((float)(u[0] - u[3]), (float)(u[1] - u[3]),
-                                         (float)(u[2] - u[3]), (float)(u[4] - u[3]),
-                                         (float)(u[5] - u[3]), (float)(u[6] - u[3]));
-    else
+        for (int k = -3; k <= 3; ++k) {
+            if (k == 0) continue;
+            const long long j = i + k * dir;
+            if constexpr (YPLUS)
+                d[k + 3] = (float)(ld_nc(Y + j) - y0) + ((float)ld_nc(X + j) - x0);
+            else
+                d[k + 3] = (float)((double)ld_nc(X + j) - y0);
+        }
+        const float corr = weno7_corr(d[0], d[1], d[2], d[4], d[5], d[6]);
+        return y0 + (double)(x0 + corr);
+    } else {
+        double u[7];
+#pragma unroll
+        for (int k = -3; k <= 3; ++k) u[k + 3] = in_at<YPLUS>(X, Y, i + k * dir);
         return weno7_face(u[0], u[1], u[2], u[3], u[4], u[5], u[6]);
+    }
 }
 
 // FD advection (src/rhs_fd.hpp:53-73) and Kreiss-Oliger dissipation

@@ -161,7 +161,9 @@ __device__ __forceinline__ void consumer_sync()
 // the own-cell tiles A (and B).
 template <class TIN, class TOUT, int STAGE> struct Layout {
     static constexpr bool INC = inc_form<TIN, TOUT>();
-    static constexpr int XW = xw<TIN>();
+    // FP64 stage 3 streams the most bytes per chunk: its 40-cell rows keep a
+    // two-buffer ring within half an SM's shared memory (two blocks per SM)
+    static constexpr int XW = (!INC && STAGE == 3) ? TZ + 2 * HALO : xw<TIN>();
     static constexpr int XB = NCOMP * R * XW * (int)sizeof(TIN);
     // Y: FP64 stages 2-3 read it at their own cells; FP32-bulk stages 2-4 read
     // it with the halo (their input is Y + D)
@@ -398,14 +400,25 @@ __global__ void __launch_bounds__(tma::NTHR, MINB)
                 else
                     return (double)xrow[q * XW + j];
             };
+            // FP32-bulk: the stencil difference u(j + k) - u(j) as
+            // (Y difference in FP64, rounded) + (D difference in FP32)
+            auto dif = [&](int q, int j, int k) -> float {
+                if constexpr (INC && STAGE >= 2)
+                    return (float)(yrow[q * YW + j + k] - yrow[q * YW + j]) +
+                           ((float)xrow[q * XW + j + k] - (float)xrow[q * XW + j]);
+                else
+                    return (float)((double)xrow[q * XW + j + k] - (double)xrow[q * XW + j]);
+            };
             // upwind WENO7 face of component q about cell j, stencil direction dir
             auto face = [&](int q, int j, int dir) -> double {
                 if constexpr (INC) {
-                    const double u = in(q, j);
-                    return u + (double)weno7_corr(
-                                   (float)(in(q, j - 3 * dir) - u), (float)(in(q, j - 2 * dir) - u),
-                                   (float)(in(q, j - dir) - u), (float)(in(q, j + dir) - u),
-                                   (float)(in(q, j + 2 * dir) - u), (float)(in(q, j + 3 * dir) - u));
+                    const float corr = weno7_corr(dif(q, j, -3 * dir), dif(q, j, -2 * dir),
+                                                  dif(q, j, -dir), dif(q, j, dir),
+                                                  dif(q, j, 2 * dir), dif(q, j, 3 * dir));
+                    if constexpr (STAGE >= 2)  // Y + (D + correction)
+                        return yrow[q * YW + j] + (double)((float)xrow[q * XW + j] + corr);
+                    else
+                        return (double)xrow[q * XW + j] + (double)corr;
                 } else {
                     return weno7_face(in(q, j - 3 * dir), in(q, j - 2 * dir), in(q, j - dir),
                                       in(q, j), in(q, j + dir), in(q, j + 2 * dir),
@@ -804,7 +817,19 @@ static int tma_minb_env()
     return v;
 }
 
-int tma_blocks_per_sm(int scheme) { return scheme == FV ? tma_minb_env() : 1; }
+// FD: COSENU_TMA_MINB_FD=2 runs two blocks per SM (<= 112 registers each,
+// half the shared memory) instead of one.
+static int tma_minb_fd_env()
+{
+    static int v = -1;
+    if (v < 0) {
+        const char *e = getenv("COSENU_TMA_MINB_FD");
+        v = (e && e[0] == '2') ? 2 : 1;
+    }
+    return v;
+}
+
+int tma_blocks_per_sm(int scheme) { return scheme == FV ? tma_minb_env() : tma_minb_fd_env(); }
 
 template <int SCHEME, bool GEN, int STAGE, class TIN, class TOUT>
 static cudaError_t launch_one(const StageMaps &m, const StageArgs &a, int *err, int nblocks,
@@ -816,7 +841,16 @@ static cudaError_t launch_one(const StageMaps &m, const StageArgs &a, int *err, 
             cudaError_t e = LNB(2, 1);
             if (e == cudaSuccess) e = LNB(3, 1);
             if (e == cudaSuccess) e = LNB(4, 1);
+            if (e == cudaSuccess) e = LNB(2, 2);
+            if (e == cudaSuccess) e = LNB(3, 2);
+            if (e == cudaSuccess) e = LNB(4, 2);
             return e;
+        }
+        if (tma_minb_fd_env() == 2) {
+            const int lim = tma_smem_limit(2);
+            if (tma_smem<TIN, TOUT, STAGE>(4) <= lim) return LNB(4, 2);
+            if (tma_smem<TIN, TOUT, STAGE>(3) <= lim) return LNB(3, 2);
+            return LNB(2, 2);
         }
         switch (tma_fd_ring<TIN, TOUT, STAGE>()) {
         case 2: return LNB(2, 1);

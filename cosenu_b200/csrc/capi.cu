@@ -105,7 +105,13 @@ void choose_tile(cosenu_ctx *ctx, int layout = 0)
     }
     int tz = p.tile_z;
     if (tz == 0) tz = (p.nz % 32 == 0) ? 32 : (p.nz % 16 == 0 ? 16 : 8);
-    int rp = NTHREADS / tz;
+    // small grids: split each cell's components over `split` threads
+    // (COSENU_SPLIT=2|4 with 32-cell z tiles and an automatic v tile)
+    int split = 1;
+    const char *se = getenv("COSENU_SPLIT");
+    if (se && (se[0] == '2' || se[0] == '4') && tz == 32 && p.tile_v == 0) split = se[0] - '0';
+    ctx->split = split;
+    int rp = NTHREADS / tz / split;
     int tv = p.tile_v;
     if (tv == 0) {
         tv = std::min(p.nvz, 64);
@@ -209,7 +215,7 @@ cudaError_t launch_stage(cosenu_ctx *ctx, int stage, cudaStream_t s)
         e = launch_rk4_stage_tma(*mX, *mY, *mA, *mB, a, ctx->p.scheme, stage, ctx->fp32,
                                  ctx->err_flag, nblk, s);
     } else {
-        e = launch_rk4_stage(a, ctx->p.scheme, stage, ctx->tz, ctx->fp32, s);
+        e = launch_rk4_stage(a, ctx->p.scheme, stage, ctx->tz, ctx->fp32, s, ctx->split);
     }
     if (e == cudaSuccess && stage == 4) flip(ctx);
     return e;
@@ -542,6 +548,7 @@ int ctx_set_tiling(cosenu_ctx *ctx, int tz, int tv)
         ctx->tz = tz;
         ctx->tv = tv;
         ctx->nvt = nvt;
+        ctx->split = 1;
         ctx->use_tma = false;
     }
     drop_graphs(ctx);

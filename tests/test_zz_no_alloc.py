@@ -44,6 +44,10 @@ T32x16 = dict(tile_z=32, tile_v=16)
     # the default v tile (min(nvz, 64)) and a collective-term-free run
     (dict(FD_SMALL, nvz=96), {}, 0),
     (dict(FD_SMALL, coll=False), T32x16, 0),
+    # FP32-bulk: the increments and the second state buffer in the scratch
+    (dict(FD_SMALL, precision="fp32"), T32x16, 0),
+    (dict(scheme="fv", nz=256, nvz=20, gz=4, omega=1e-2, theta_deg=37.0, z0=-128.0, z1=128.0,
+          precision="fp32"), T32x16, 0),
     # the upwind FD stencil (its row factors come from the scratch tables)
     (dict(FD_SMALL, fd_advec="upwind", ko_order=5, gz=3), dict(tile_z=16, tile_v=5), 0),
     # rows of the caller's tensor padded past nz (row pitch ld = nz + 8)

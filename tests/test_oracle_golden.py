@@ -153,3 +153,18 @@ def test_oracle_c1_after_saturation(oracle):
     pee, pbee = oracle.pee_v(case, y, st0)
     assert np.abs(pee - d["rho_1500_pee_v"]).max() <= 1e-6
     assert np.abs(pbee - d["rho_1500_pbee_v"]).max() <= 1e-6
+
+
+def test_oracle_fd_benchmark_grid_against_reference_run(oracle):
+    """The oracle on the full FD benchmark grid (nz 32768 x nvz 256), 5 steps,
+    against the reference's own dump: the stored columns to 1e-14 and the
+    per-row checksums of the whole state to 1e-11 relative."""
+    case, d = load_golden("c2_ref")
+    G, bG, st0 = oracle.init_seeded(case, seed=int(d["seed"]))
+    assert hashlib.sha256(st0[..., case.gz:case.gz + case.nz].tobytes()).hexdigest() == \
+        str(d["state0_sha256"])
+    s = oracle.step(case, st0, 5, nthreads=os.cpu_count() or 1)[..., case.gz:case.gz + case.nz]
+    assert np.abs(s[:, :, d["columns"]] - d["rho_5_columns"]).max() <= 1e-14
+    ck = np.stack([s.sum(axis=2), (s * s).sum(axis=2), np.abs(s).sum(axis=2)], -1)
+    want = d["rho_5_row_checksums"]
+    assert np.all(np.abs(ck - want) <= 1e-11 * np.abs(want) + 1e-13 * case.nz)

@@ -491,6 +491,58 @@ def run_ensemble(args):
     print(json.dumps(line), flush=True)
 
 
+def run_divergence_study(args):
+    """Where in time the ensemble's final-P_ee difference comes from: for every
+    32nd member of the ensemble workload, three runs of the same seeded set-up
+    to t = 1000/mu -- FP64 (default kernel), FP64 with a different velocity-moment
+    summation order (register-tiled kernel, 16 x 8 tiles: the same arithmetic up
+    to rounding), and FP32-bulk -- with <P_ee> every 1/200 of the run.  Reports the
+    saturation time (first |1 - <P_ee>| > 1e-2) and the first time each
+    difference from the FP64 run exceeds 1e-6."""
+    import torch
+
+    from cosenu_b200 import NuOsc
+    from cosenu_b200.ensemble import ensemble_instances
+
+    torch.cuda.set_device(0)
+    xs = ensemble_instances(args.instances, t_factor=args.t_factor)
+    out = []
+    for i in range(0, len(xs), 32):
+        x = xs[i]
+        runs = {}
+        for name, kw in (("fp64", {}), ("fp64_reordered", {"tile_z": 16, "tile_v": 8}),
+                         ("fp32_bulk", {"precision": "fp32"})):
+            sim = NuOsc(nz=x.nz, nvz=x.nvz, gz=4, z0=x.z0, z1=x.z1, cfl=x.cfl, omega=0.0,
+                        mu=x.mu, scheme="fv", **kw)
+            sim.init_seeded(x.seed, instance=x.index, sig_nu=x.sig_nu, sig_nubar=x.sig_nubar,
+                            alpha=x.alpha)
+            k = max(1, x.nsteps // 200)
+            t, done, pee = [], 0, []
+            while done < x.nsteps:
+                n = min(k, x.nsteps - done)
+                sim.evolve(n)
+                done += n
+                t.append(done * sim.dt)
+                pee.append(sim.analyse()["Pee"])
+            sim.close()
+            runs[name] = (t, pee)
+        t, p64 = runs["fp64"]
+        t_sat = next((tt for tt, p in zip(t, p64) if abs(1.0 - p) > 1e-2), None)
+        rec = {"member": i, "nz": x.nz, "nvz": x.nvz, "mu": x.mu, "t_end": t[-1],
+               "t_saturation": t_sat, "final_Pee_fp64": p64[-1]}
+        for name in ("fp64_reordered", "fp32_bulk"):
+            d = [abs(a - b) for a, b in zip(runs[name][1], p64)]
+            rec[f"{name}_final_diff"] = d[-1]
+            rec[f"{name}_max_diff"] = max(d)
+            rec[f"{name}_t_diff_gt_1e-6"] = next((tt for tt, e in zip(t, d) if e > 1e-6), None)
+            rec[f"{name}_max_diff_before_saturation"] = max(
+                [e for tt, e in zip(t, d) if t_sat is None or tt < t_sat] or [0.0])
+        out.append(rec)
+        print(json.dumps(rec), flush=True)
+    print(json.dumps({"study": "P_ee divergence in the ensemble workload", "members": out}),
+          flush=True)
+
+
 def run_fp32_study(args):
     """FV at 65536 x 512: the FP32-bulk form against the FP64 form on the same seeded
     input: max-abs error per component at the end, <Pee>(t) error, trace and
@@ -738,6 +790,9 @@ def main():
                     help="cost of a snapshot every --snapshot-every steps, asynchronous vs "
                          "blocking, on the chosen workload")
     ap.add_argument("--snapshot-every", type=int, default=100)
+    ap.add_argument("--divergence-study", action="store_true",
+                    help="c4: <P_ee>(t) of FP64, reordered FP64 and FP32-bulk runs of "
+                         "every 32nd member")
     ap.add_argument("--t-factor", type=float, default=1000.0, help="c4: run to t_factor/mu")
     ap.add_argument("--workload", choices=sorted(WORKLOADS) + ["c4", "c5"], default="c2",
                     help="c2 (default, the headline): FD 32768 x 256; c1: FV 1024 x 64; "
@@ -748,7 +803,10 @@ def main():
                          "workload is nz = 32768)")
     args = ap.parse_args()
     if args.workload == "c4":
-        run_ensemble(args)
+        if args.divergence_study:
+            run_divergence_study(args)
+        else:
+            run_ensemble(args)
         return
     if args.workload == "c5":
         run_surrogate(args)

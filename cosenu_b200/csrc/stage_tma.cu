@@ -507,23 +507,6 @@ __global__ void __launch_bounds__(tma::NTHR, MINB)
                 // for after the collective term (the reference's order)
 #pragma unroll
                 for (int q = 0; q < NCOMP; ++q) {
-                    if constexpr (INC && STAGE >= 2 && !GEN) {
-                        // FP32-bulk central FD4 + KO3 on Y + D: both stencils are
-                        // linear, so the Y part is taken in FP64 and the D part in
-                        // FP32, joined once per term
-                        const double *yq = yrow + q * YW + lane;
-                        const TIN *dq = xrow + q * XW + lane;
-                        const double ym2 = yq[-2], ym1 = yq[-1], yc = yq[0], yp1 = yq[1],
-                                     yp2 = yq[2];
-                        const float dm2 = dq[-2], dm1 = dq[-1], dc = dq[0], dp1 = dq[1],
-                                    dp2 = dq[2];
-                        if (advec)
-                            o[q] += factor * (((ym2 - yp2) - 8.0 * (ym1 - yp1)) +
-                                              (double)((dm2 - dp2) - 8.f * (dm1 - dp1)));
-                        ko[q] = ko_eps * ((ym2 + yp2 - 4.0 * (ym1 + yp1) + 6.0 * yc) +
-                                          (double)(dm2 + dp2 - 4.f * (dm1 + dp1) + 6.f * dc));
-                        continue;
-                    }
                     const double m2 = in(q, lane - 2), m1 = in(q, lane - 1), p1 = in(q, lane + 1),
                                  p2 = in(q, lane + 2);
                     if (advec) {

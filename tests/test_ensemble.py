@@ -51,12 +51,16 @@ def _standalone(x, i, scheme, precision, **kw):
 
 
 @pytest.mark.gpu
+@pytest.mark.parametrize("precision", ["fp64", "fp32"])
 @pytest.mark.parametrize("scheme", ["fv", "fd"])
-def test_ensemble_tma_matches_members_run_alone(gpu_lib, monkeypatch, scheme):
+def test_ensemble_tma_matches_members_run_alone(gpu_lib, monkeypatch, scheme, precision):
+    """FP32-bulk members alternate their two state buffers every step, so the
+    ensemble launches use per-parity argument and tensor-map sets: odd and even
+    step counts (5..39) and phases of both parities are covered."""
     from cosenu_b200.ensemble import Ensemble
     xs = _small()
     monkeypatch.setenv("COSENU_KERNEL", "tma")  # standalone runs use the same kernel family
-    with Ensemble(xs, scheme=scheme) as ens:
+    with Ensemble(xs, scheme=scheme, precision=precision) as ens:
         assert ens.config()["use_tma"]
         ens.init_seeded()
         ens.run()
@@ -64,7 +68,7 @@ def test_ensemble_tma_matches_members_run_alone(gpu_lib, monkeypatch, scheme):
         for i, (x, m) in enumerate(zip(xs, ens.members)):
             assert m.steps == x.nsteps
             got = m.download()
-            want = _standalone(x, i, scheme, "fp64")
+            want = _standalone(x, i, scheme, precision)
             assert np.abs(got - want).max() <= 1e-13, i
 
 
@@ -131,8 +135,9 @@ def test_ensemble_fp32_bulk_close_to_fp64(gpu_lib):
             ens.run()
             ens.synchronize()
             outs.append([m.download() for m in ens.members])
+    # 5-40 steps before saturation: the increment form stays within 1e-9 of FP64
     for a, b in zip(*outs):
-        assert np.abs(a - b).max() <= 1e-5
+        assert np.abs(a - b).max() <= 1e-9
 
 
 @pytest.mark.gpu

@@ -105,13 +105,7 @@ void choose_tile(cosenu_ctx *ctx, int layout = 0)
     }
     int tz = p.tile_z;
     if (tz == 0) tz = (p.nz % 32 == 0) ? 32 : (p.nz % 16 == 0 ? 16 : 8);
-    // small grids: split each cell's components over `split` threads
-    // (COSENU_SPLIT=2|4 with 32-cell z tiles and an automatic v tile)
-    int split = 1;
-    const char *se = getenv("COSENU_SPLIT");
-    if (se && (se[0] == '2' || se[0] == '4') && tz == 32 && p.tile_v == 0) split = se[0] - '0';
-    ctx->split = split;
-    int rp = NTHREADS / tz / split;
+    int rp = NTHREADS / tz;
     int tv = p.tile_v;
     if (tv == 0) {
         tv = std::min(p.nvz, 64);
@@ -215,7 +209,7 @@ cudaError_t launch_stage(cosenu_ctx *ctx, int stage, cudaStream_t s)
         e = launch_rk4_stage_tma(*mX, *mY, *mA, *mB, a, ctx->p.scheme, stage, ctx->fp32,
                                  ctx->err_flag, nblk, s);
     } else {
-        e = launch_rk4_stage(a, ctx->p.scheme, stage, ctx->tz, ctx->fp32, s, ctx->split);
+        e = launch_rk4_stage(a, ctx->p.scheme, stage, ctx->tz, ctx->fp32, s);
     }
     if (e == cudaSuccess && stage == 4) flip(ctx);
     return e;
@@ -489,19 +483,19 @@ int ctx_create(const cosenu_params *pp, cosenu_ctx **out, int layout)
     cudaMemsetAsync(ctx->err_flag, 0, 64, ctx->stream);
     if (ctx->use_tma) {
         const int ub = ctx->fp32 ? 4 : 8, bx = tma_box_x(8), bxu = tma_box_x(ub),
-                  bt = tma_box_tile();
-        int r = make_state_map(&ctx->mYb40[0], ctx->Yb[0], 8, ctx->ld, p.nvz, ctx->cs, bx);
-        if (!r) r = make_state_map(&ctx->mYb40[1], ctx->Yb[1], 8, ctx->ld, p.nvz, ctx->cs, bx);
-        if (!r) r = make_state_map(&ctx->mU0_40, ctx->U0, ub, ctx->ld, p.nvz, ctx->cs, bxu);
+                  bt = tma_box_tile(), br = tma_box_rows(p.scheme);
+        int r = make_state_map(&ctx->mYb40[0], ctx->Yb[0], 8, ctx->ld, p.nvz, ctx->cs, bx, br);
+        if (!r) r = make_state_map(&ctx->mYb40[1], ctx->Yb[1], 8, ctx->ld, p.nvz, ctx->cs, bx, br);
+        if (!r) r = make_state_map(&ctx->mU0_40, ctx->U0, ub, ctx->ld, p.nvz, ctx->cs, bxu, br);
         // (FP64 stage 3 reads U1 in 40-cell rows, see the TMA kernel's Layout)
         if (!r) r = make_state_map(&ctx->mU1_40, ctx->U1, ub, ctx->ld, p.nvz, ctx->cs,
-                                   ctx->fp32 ? bxu : bt + 8);
-        if (!r) r = make_state_map(&ctx->mY32, ctx->Yb[0], 8, ctx->ld, p.nvz, ctx->cs, bt);
-        if (!r) r = make_state_map(&ctx->mA32, ctx->Yb[1], 8, ctx->ld, p.nvz, ctx->cs, bt);
-        if (!r) r = make_state_map(&ctx->mU0_32, ctx->U0, ub, ctx->ld, p.nvz, ctx->cs, bt);
-        if (!r) r = make_state_map(&ctx->mU1_32, ctx->U1, ub, ctx->ld, p.nvz, ctx->cs, bt);
+                                   ctx->fp32 ? bxu : bt + 8, br);
+        if (!r) r = make_state_map(&ctx->mY32, ctx->Yb[0], 8, ctx->ld, p.nvz, ctx->cs, bt, br);
+        if (!r) r = make_state_map(&ctx->mA32, ctx->Yb[1], 8, ctx->ld, p.nvz, ctx->cs, bt, br);
+        if (!r) r = make_state_map(&ctx->mU0_32, ctx->U0, ub, ctx->ld, p.nvz, ctx->cs, bt, br);
+        if (!r) r = make_state_map(&ctx->mU1_32, ctx->U1, ub, ctx->ld, p.nvz, ctx->cs, bt, br);
         if (!r && ctx->U2)
-            r = make_state_map(&ctx->mU2_40, ctx->U2, ub, ctx->ld, p.nvz, ctx->cs, bxu);
+            r = make_state_map(&ctx->mU2_40, ctx->U2, ub, ctx->ld, p.nvz, ctx->cs, bxu, br);
         if (!ctx->U2) ctx->mU2_40 = ctx->mU1_40;  // unused in FP64
         if (!r && tma_prepare() != cudaSuccess) r = -2;
         if (r) {
@@ -548,7 +542,6 @@ int ctx_set_tiling(cosenu_ctx *ctx, int tz, int tv)
         ctx->tz = tz;
         ctx->tv = tv;
         ctx->nvt = nvt;
-        ctx->split = 1;
         ctx->use_tma = false;
     }
     drop_graphs(ctx);

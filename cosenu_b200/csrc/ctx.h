@@ -12,13 +12,14 @@
 
 namespace cosenu {
 cudaError_t launch_rk4_stage(const StageArgs &a, int scheme, int stage, int tz, int fp32,
-                             cudaStream_t s, int split = 1);
+                             cudaStream_t s);
 cudaError_t launch_ghost_fill(double *buf, long long cs, int ld, int nz, int nvz, int H, int bc,
                               cudaStream_t s);
 cudaError_t launch_moments(const double *X, double *M, const double *vz, long long cs, int ld,
                            int nz, int nvz, int tz, int tv, cudaStream_t s);
 int make_state_map(CUtensorMap *map, const void *base, int elem_bytes, int ld, int nvz,
-                   long long cs, int box_cells);
+                   long long cs, int box_cells, int box_rows);
+int tma_box_rows(int scheme);
 int tma_box_x(int elem_bytes);
 int tma_box_tile();
 int tma_max_nvz();
@@ -39,7 +40,6 @@ cudaError_t launch_rk4_stage_batch(const BatchDev &bd, int scheme, int stage, in
 struct cosenu_ctx {
     cosenu_params p{};
     int ld = 0, H = 4, tz = 32, tv = 64, nvt = 1;
-    int split = 1;  // register-tiled kernel: threads per cell (component groups)
     long long cs = 0;
     double dz = 0, dv = 0, dt = 0, ct = 0, st = 0;
     int fp32 = 0;

@@ -40,7 +40,7 @@ extern thread_local std::string g_create_error;
 
 namespace cosenu {
 cudaError_t launch_rk4_stage(const StageArgs &a, int scheme, int stage, int tz, int fp32,
-                             cudaStream_t s, int split);
+                             cudaStream_t s);
 cudaError_t launch_ghost_fill(double *buf, long long cs, int ld, int nz, int nvz, int H, int bc,
                               cudaStream_t s);
 cudaError_t launch_moments(const double *X, double *M, const double *vz, long long cs, int ld,
@@ -275,7 +275,7 @@ extern "C" int cosenu_step_noalloc(const cosenu_params *pp, double *const state[
                 case 4: a.X = D3; a.U = ynext; a.Min = M[0]; a.Mout = M[2]; break;
                 }
             }
-            if ((e = launch_rk4_stage(a, p.scheme, st, tz, fp32, s, 1)) != cudaSuccess)
+            if ((e = launch_rk4_stage(a, p.scheme, st, tz, fp32, s)) != cudaSuccess)
                 return done(COSENU_ERR_CUDA, "stage", e);
         }
         if (fp32) std::swap(ycur, ynext);

@@ -15,10 +15,7 @@
 // Thread (lz, rr) owns column z0+lz and rows rr, rr+RP, ... (RP = 256/TZ);
 // the TZ lanes of one row segment sit in one warp, so z-neighbour values move
 // by warp shuffle.  Loads of the stencil go through L1 (the same 128-byte
-// lines serve all lanes of a segment).  On small grids S > 1 warps share a
-// row segment (TZ = 32): warp w takes the 8/S components of group w % S, so
-// S times as many threads work on the grid (each still reads all 8 of its
-// cell's values for the source terms).
+// lines serve all lanes of a segment).
 //
 // FV: only the upwind WENO7 reconstruction is evaluated (sign(v) is uniform
 // along a row); each lane computes the one face it owns, takes the other from
@@ -118,14 +115,12 @@ __device__ __forceinline__ void fd_terms(const TIN *__restrict__ X, const double
 }
 
 // ---------------------------------------------------------------------------
-template <int SCHEME, int STAGE, int TZ, int S, class TIN, class TOUT, bool BATCHED>
+template <int SCHEME, int STAGE, int TZ, class TIN, class TOUT, bool BATCHED>
 __global__ void __launch_bounds__(NTHREADS, 2)
     rk4_stage_kernel(const __grid_constant__ StageArgs a0, const BatchDev bd)
 {
     constexpr bool INC = inc_form<TIN, TOUT>();
     constexpr bool YPLUS = INC && STAGE >= 2;
-    static_assert(S == 1 || TZ == 32, "component groups need whole-warp row segments");
-    constexpr int CPT = NCOMP / S;  // components per thread
     // tile: (z tile, v tile) from the grid, or (instance, z tile, v tile) from
     // the ensemble table
     int zt = blockIdx.x, vt = blockIdx.y, inst = 0;
@@ -136,10 +131,9 @@ __global__ void __launch_bounds__(NTHREADS, 2)
         vt = e.z;
     }
     const StageArgs &a = BATCHED ? bd.args[inst * 4 + STAGE - 1] : a0;
-    constexpr int NSLOT = NTHREADS / TZ;  // row segments of the block
-    constexpr int RP = NSLOT / S;         // rows per pass
+    constexpr int RP = NTHREADS / TZ;
     __shared__ double s_mom[NMOM][TZ];
-    __shared__ double s_red[NSLOT][NMOM][TZ];
+    __shared__ double s_red[RP][NMOM][TZ];
     __shared__ double s_edge[SCHEME == FV ? MAX_TV : 1][NCOMP];
 
     const TIN *__restrict__ X = static_cast<const TIN *>(a.X);
@@ -147,10 +141,7 @@ __global__ void __launch_bounds__(NTHREADS, 2)
     TOUT *__restrict__ U = static_cast<TOUT *>(a.U);
     const int tid = threadIdx.x;
     const int lz = tid % TZ;
-    const int slot = tid / TZ;
-    const int grp = slot % S;  // component group of this warp
-    const int rr = slot / S;
-    auto own = [&](int k) { return S == 1 || k / CPT == grp; };
+    const int rr = tid / TZ;
     const int z0 = zt * TZ;
     const int z = z0 + lz;
     const int vbeg = vt * a.tv;
@@ -214,7 +205,7 @@ __global__ void __launch_bounds__(NTHREADS, 2)
 #pragma unroll
             for (int k = 0; k < NCOMP; ++k) {
                 double adv = 0.0;
-                if (advec && own(k)) {
+                if (advec) {
                     double fown = face_at<INC, YPLUS>(X, Yb, k * a.cs + rowoff, dir);
                     double fnb = shfl_idx(fown, src < 0 ? 0 : (src >= TZ ? TZ - 1 : src), TZ);
                     double fm1 = shfl_idx(fown, lz > 0 ? lz - 1 : 0, TZ);
@@ -246,12 +237,9 @@ __global__ void __launch_bounds__(NTHREADS, 2)
             double adv[NCOMP], ko[NCOMP];
             const int sv = (vzv > 0.0) - (vzv < 0.0);
 #pragma unroll
-            for (int k = 0; k < NCOMP; ++k) {
-                adv[k] = ko[k] = 0.0;
-                if (own(k))
-                    fd_terms<YPLUS>(X, Yb, k * a.cs + rowoff, a.fd_advec, a.ko_order, sv, rowfac,
-                                    a.ko_eps, advec, adv[k], ko[k]);
-            }
+            for (int k = 0; k < NCOMP; ++k)
+                fd_terms<YPLUS>(X, Yb, k * a.cs + rowoff, a.fd_advec, a.ko_order, sv, rowfac,
+                                a.ko_eps, advec, adv[k], ko[k]);
 #pragma unroll
             for (int k = 0; k < NCOMP; ++k) o[k] = 0.0;
             if (a.flags & F_VAC) {
@@ -325,9 +313,6 @@ __global__ void __launch_bounds__(NTHREADS, 2)
         double um[NCOMP];  // the output as a stage value (for the moments)
 #pragma unroll
         for (int k = 0; k < NCOMP; ++k) {
-            u[k] = TOUT(0);
-            um[k] = 0.0;
-            if (!own(k)) continue;
             const double kk = o[k];
             const long long idx = k * a.cs + rowoff;
             if constexpr (INC) {
@@ -370,7 +355,6 @@ __global__ void __launch_bounds__(NTHREADS, 2)
         if (valid) {
 #pragma unroll
             for (int k = 0; k < NCOMP; ++k) {
-                if (!own(k)) continue;
                 TOUT *row = U + k * a.cs + (long long)v * a.ld + HP;
                 row[z] = u[k];
                 if (!open_bc) {
@@ -391,7 +375,6 @@ __global__ void __launch_bounds__(NTHREADS, 2)
                 }
             }
             if (coll) {
-                // this thread's components' share (the others are zero here)
                 const double Am = um[EXI] + um[BEXI];
                 const double Bm = um[EXR] - um[BEXR];
                 const double Cm = um[EE] - um[XX] - um[BEE] + um[BXX];
@@ -407,13 +390,13 @@ __global__ void __launch_bounds__(NTHREADS, 2)
 
     if (coll) {
 #pragma unroll
-        for (int m = 0; m < NMOM; ++m) s_red[slot][m][lz] = macc[m];
+        for (int m = 0; m < NMOM; ++m) s_red[rr][m][lz] = macc[m];
         __syncthreads();
         for (int q = tid; q < NMOM * TZ; q += NTHREADS) {
             int m = q / TZ, zz = q % TZ;
             double s = 0.0;
 #pragma unroll 4
-            for (int t = 0; t < NSLOT; ++t) s += s_red[t][m][zz];
+            for (int t = 0; t < RP; ++t) s += s_red[t][m][zz];
             a.Mout[((long long)vt * NMOM + m) * a.nz + z0 + zz] = s;
         }
     }
@@ -422,7 +405,7 @@ __global__ void __launch_bounds__(NTHREADS, 2)
 // ---------------------------------------------------------------------------
 // host launcher
 
-template <int SCHEME, int TZ, int S, bool B>
+template <int SCHEME, int TZ, bool B>
 static cudaError_t launch_p(const StageArgs &a, int stage, int fp32, cudaStream_t s,
                             const BatchDev &bd)
 {
@@ -431,18 +414,18 @@ static cudaError_t launch_p(const StageArgs &a, int stage, int fp32, cudaStream_
     if (fp32) {
         // FP32-bulk: Y in, D1 out; Y + D1 in, D2 out; Y + D2 in, D3 out; Y + D3 in, Y' out
         switch (stage) {
-        case 1: rk4_stage_kernel<SCHEME, 1, TZ, S, double, float, B><<<grid, block, 0, s>>>(a, bd); break;
-        case 2: rk4_stage_kernel<SCHEME, 2, TZ, S, float, float, B><<<grid, block, 0, s>>>(a, bd); break;
-        case 3: rk4_stage_kernel<SCHEME, 3, TZ, S, float, float, B><<<grid, block, 0, s>>>(a, bd); break;
-        case 4: rk4_stage_kernel<SCHEME, 4, TZ, S, float, double, B><<<grid, block, 0, s>>>(a, bd); break;
+        case 1: rk4_stage_kernel<SCHEME, 1, TZ, double, float, B><<<grid, block, 0, s>>>(a, bd); break;
+        case 2: rk4_stage_kernel<SCHEME, 2, TZ, float, float, B><<<grid, block, 0, s>>>(a, bd); break;
+        case 3: rk4_stage_kernel<SCHEME, 3, TZ, float, float, B><<<grid, block, 0, s>>>(a, bd); break;
+        case 4: rk4_stage_kernel<SCHEME, 4, TZ, float, double, B><<<grid, block, 0, s>>>(a, bd); break;
         default: return cudaErrorInvalidValue;
         }
     } else {
         switch (stage) {
-        case 1: rk4_stage_kernel<SCHEME, 1, TZ, S, double, double, B><<<grid, block, 0, s>>>(a, bd); break;
-        case 2: rk4_stage_kernel<SCHEME, 2, TZ, S, double, double, B><<<grid, block, 0, s>>>(a, bd); break;
-        case 3: rk4_stage_kernel<SCHEME, 3, TZ, S, double, double, B><<<grid, block, 0, s>>>(a, bd); break;
-        case 4: rk4_stage_kernel<SCHEME, 4, TZ, S, double, double, B><<<grid, block, 0, s>>>(a, bd); break;
+        case 1: rk4_stage_kernel<SCHEME, 1, TZ, double, double, B><<<grid, block, 0, s>>>(a, bd); break;
+        case 2: rk4_stage_kernel<SCHEME, 2, TZ, double, double, B><<<grid, block, 0, s>>>(a, bd); break;
+        case 3: rk4_stage_kernel<SCHEME, 3, TZ, double, double, B><<<grid, block, 0, s>>>(a, bd); break;
+        case 4: rk4_stage_kernel<SCHEME, 4, TZ, double, double, B><<<grid, block, 0, s>>>(a, bd); break;
         default: return cudaErrorInvalidValue;
         }
     }
@@ -450,34 +433,29 @@ static cudaError_t launch_p(const StageArgs &a, int stage, int fp32, cudaStream_
 }
 
 template <bool B>
-static cudaError_t launch_s(const StageArgs &a, int scheme, int stage, int tz, int split, int fp32,
-                           cudaStream_t s, const BatchDev &bd)
+static cudaError_t launch_s(const StageArgs &a, int scheme, int stage, int tz, int fp32,
+                            cudaStream_t s, const BatchDev &bd)
 {
     if (scheme == FV) {
-        switch (tz * 8 + split) {
-        case 8 * 8 + 1: return launch_p<FV, 8, 1, B>(a, stage, fp32, s, bd);
-        case 16 * 8 + 1: return launch_p<FV, 16, 1, B>(a, stage, fp32, s, bd);
-        case 32 * 8 + 1: return launch_p<FV, 32, 1, B>(a, stage, fp32, s, bd);
-        case 32 * 8 + 2: return launch_p<FV, 32, 2, B>(a, stage, fp32, s, bd);
-        case 32 * 8 + 4: return launch_p<FV, 32, 4, B>(a, stage, fp32, s, bd);
+        switch (tz) {
+        case 8: return launch_p<FV, 8, B>(a, stage, fp32, s, bd);
+        case 16: return launch_p<FV, 16, B>(a, stage, fp32, s, bd);
+        case 32: return launch_p<FV, 32, B>(a, stage, fp32, s, bd);
         }
     } else {
-        switch (tz * 8 + split) {
-        case 8 * 8 + 1: return launch_p<FD, 8, 1, B>(a, stage, fp32, s, bd);
-        case 16 * 8 + 1: return launch_p<FD, 16, 1, B>(a, stage, fp32, s, bd);
-        case 32 * 8 + 1: return launch_p<FD, 32, 1, B>(a, stage, fp32, s, bd);
-        case 32 * 8 + 2: return launch_p<FD, 32, 2, B>(a, stage, fp32, s, bd);
-        case 32 * 8 + 4: return launch_p<FD, 32, 4, B>(a, stage, fp32, s, bd);
+        switch (tz) {
+        case 8: return launch_p<FD, 8, B>(a, stage, fp32, s, bd);
+        case 16: return launch_p<FD, 16, B>(a, stage, fp32, s, bd);
+        case 32: return launch_p<FD, 32, B>(a, stage, fp32, s, bd);
         }
     }
     return cudaErrorInvalidValue;
 }
 
-// split: threads per cell (1; or 2, 4 with tz 32), each with 8/split components
 cudaError_t launch_rk4_stage(const StageArgs &a, int scheme, int stage, int tz, int fp32,
-                             cudaStream_t s, int split)
+                             cudaStream_t s)
 {
-    return launch_s<false>(a, scheme, stage, tz, split, fp32, s, BatchDev{});
+    return launch_s<false>(a, scheme, stage, tz, fp32, s, BatchDev{});
 }
 
 // Ensemble launch: one block per table entry (instance, z tile, v tile); the
@@ -486,7 +464,7 @@ cudaError_t launch_rk4_stage_batch(const BatchDev &bd, int scheme, int stage, in
                                    cudaStream_t s)
 {
     StageArgs a{};
-    return launch_s<true>(a, scheme, stage, tz, 1, fp32, s, bd);
+    return launch_s<true>(a, scheme, stage, tz, fp32, s, bd);
 }
 
 }  // namespace cosenu

@@ -50,9 +50,11 @@ constexpr int HALO = 4;          // cells each side in the input box
 // the same cell of all 8 components at once (42 doubles = 84 words: banks
 // 0, 20, 8, 28, ... for components 0..7; 44 floats = 44 words: 0, 12, 24, ...).
 template <class T> constexpr int xw() { return sizeof(T) == 8 ? 42 : 44; }
-constexpr int R = 8;             // rows per chunk = consumer warps
-constexpr int NCONS = R * 32;    // consumer threads
-constexpr int NTHR = NCONS + 32; // + producer warp
+// v rows per chunk = consumer warps.  FV runs two blocks per SM (<= 96
+// registers per thread) with 8; FD, one block per SM bound by latency more than
+// by its FP64 work, runs 12 (still ~160 registers per thread) to hide it.
+template <int SCHEME> constexpr int rows() { return SCHEME == FV ? 8 : 12; }
+template <int SCHEME> constexpr int nthr() { return rows<SCHEME>() * 32 + 32; }  // + producer
 // tensor maps per ensemble member (MapIdx lists them)
 constexpr int NMAP = 7;
 #define TMA_MAX_NVZ 1024
@@ -151,7 +153,7 @@ __device__ __forceinline__ void prefetch_map(const CUtensorMap *map)
     asm volatile("prefetch.tensormap [%0];" ::"l"((uint64_t)map) : "memory");
 }
 
-__device__ __forceinline__ void consumer_sync()
+template <int NCONS> __device__ __forceinline__ void consumer_sync()
 {
     asm volatile("bar.sync 1, %0;" ::"n"(NCONS) : "memory");
 }
@@ -159,7 +161,8 @@ __device__ __forceinline__ void consumer_sync()
 // One ring buffer holds, for R rows, boxes laid out [row][component][cell]
 // (the tensor maps put components before rows): the input box X, then Y, then
 // the own-cell tiles A (and B).
-template <class TIN, class TOUT, int STAGE> struct Layout {
+template <int SCHEME, class TIN, class TOUT, int STAGE> struct Layout {
+    static constexpr int R = rows<SCHEME>();
     static constexpr bool INC = inc_form<TIN, TOUT>();
     // FP64 stage 3 streams the most bytes per chunk: its 40-cell rows keep a
     // two-buffer ring within half an SM's shared memory (two blocks per SM)
@@ -229,7 +232,7 @@ __device__ __forceinline__ void row_values(double v0, double dv, double dz, int 
 // right-hand side is evaluated in FP64 in both forms, except the FP32-bulk
 // WENO7 weights and candidates (FP32 on FP64 stencil differences).
 template <int SCHEME, bool GEN, int STAGE, class TIN, class TOUT, int NBUF, bool BATCHED, int MINB>
-__global__ void __launch_bounds__(tma::NTHR, MINB)
+__global__ void __launch_bounds__(tma::nthr<SCHEME>(), MINB)
     rk4_stage_tma_kernel(const __grid_constant__ CUtensorMap mX,
                          const __grid_constant__ CUtensorMap mY,
                          const __grid_constant__ CUtensorMap mA,
@@ -237,7 +240,9 @@ __global__ void __launch_bounds__(tma::NTHR, MINB)
                          const __grid_constant__ StageArgs a0, int *err, const BatchDev bd)
 {
     using namespace tma;
-    using L = Layout<TIN, TOUT, STAGE>;
+    using L = Layout<SCHEME, TIN, TOUT, STAGE>;
+    constexpr int R = L::R;
+    auto consumer_sync = tma::consumer_sync<R * 32>;
     using MI = MapIdx<L::INC, STAGE>;
     constexpr bool INC = L::INC;
     extern __shared__ __align__(1024) unsigned char smem[];
@@ -704,13 +709,13 @@ static EncodeTiledFn encode_fn()
 // 3-D map over one 8-component buffer: (cells of a padded row, components,
 // rows), so that a box lands in shared memory as [row][component][cell]
 int make_state_map(CUtensorMap *map, const void *base, int elem_bytes, int ld, int nvz,
-                   long long cs, int box_cells)
+                   long long cs, int box_cells, int box_rows)
 {
     EncodeTiledFn fn = encode_fn();
     if (!fn) return -1;
     cuuint64_t dims[3] = {(cuuint64_t)ld, (cuuint64_t)NCOMP, (cuuint64_t)nvz};
     cuuint64_t strides[2] = {(cuuint64_t)cs * elem_bytes, (cuuint64_t)ld * elem_bytes};
-    cuuint32_t box[3] = {(cuuint32_t)box_cells, (cuuint32_t)NCOMP, (cuuint32_t)tma::R};
+    cuuint32_t box[3] = {(cuuint32_t)box_cells, (cuuint32_t)NCOMP, (cuuint32_t)box_rows};
     cuuint32_t es[3] = {1, 1, 1};
     CUresult r = fn(map, elem_bytes == 8 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64
                                          : CU_TENSOR_MAP_DATA_TYPE_FLOAT32,
@@ -722,6 +727,7 @@ int make_state_map(CUtensorMap *map, const void *base, int elem_bytes, int ld, i
 
 int tma_box_x(int elem_bytes) { return elem_bytes == 8 ? tma::xw<double>() : tma::xw<float>(); }
 int tma_box_tile() { return tma::TZ; }
+int tma_box_rows(int scheme) { return scheme == FV ? tma::rows<FV>() : tma::rows<FD>(); }
 // largest nvz the TMA layout is offered for (the range its tests cover; the
 // kernel itself keeps no per-row state in shared memory)
 int tma_max_nvz() { return TMA_MAX_NVZ; }
@@ -730,11 +736,11 @@ static const int TMA_SMEM_MAX = 232448;  // opt-in shared memory per block on sm
 static const int TMA_SMEM_SM = 233472;   // shared memory per SM (1 KB reserved per block)
 
 // Shared memory of one block with an NB-deep ring.
-template <class TIN, class TOUT, int STAGE>
+template <int SCHEME, class TIN, class TOUT, int STAGE>
 static int tma_smem(int NB)
 {
-    using L = tma::Layout<TIN, TOUT, STAGE>;
-    return NB * L::BUF + 2 * NB * 8 + (1 + tma::R / 2) * NMOM * tma::TZ * 8 +
+    using L = tma::Layout<SCHEME, TIN, TOUT, STAGE>;
+    return NB * L::BUF + 2 * NB * 8 + (1 + L::R / 2) * NMOM * tma::TZ * 8 +
            (int)sizeof(StageArgs);
 }
 
@@ -766,11 +772,12 @@ static cudaError_t launch_nb(const StageMaps &m, const StageArgs &a, int *err, i
         }
         return cudaSuccess;
     }
-    const int shmem = tma_smem<TIN, TOUT, STAGE>(NB);
+    const int shmem = tma_smem<SCHEME, TIN, TOUT, STAGE>(NB);
+    constexpr int NT = tma::nthr<SCHEME>();
     if (bd)
-        kernb<<<nblocks, tma::NTHR, shmem, s>>>(*m.x, *m.y, *m.a, *m.b, a, err, *bd);
+        kernb<<<nblocks, NT, shmem, s>>>(*m.x, *m.y, *m.a, *m.b, a, err, *bd);
     else
-        kern<<<nblocks, tma::NTHR, shmem, s>>>(*m.x, *m.y, *m.a, *m.b, a, err, BatchDev{});
+        kern<<<nblocks, NT, shmem, s>>>(*m.x, *m.y, *m.a, *m.b, a, err, BatchDev{});
     return cudaGetLastError();
 }
 
@@ -794,12 +801,12 @@ static int tma_ring_env()
 template <class TIN, class TOUT, int STAGE>
 static int tma_fd_ring()
 {
-    using L = tma::Layout<TIN, TOUT, STAGE>;
+    using L = tma::Layout<FD, TIN, TOUT, STAGE>;
     int nb = 2;
     while (nb < 4 && (nb + 1) * L::BUF <= 112 * 1024) ++nb;
     const int e = tma_ring_env();
     if (e) nb = e;
-    while (nb > 2 && tma_smem<TIN, TOUT, STAGE>(nb) > tma_smem_limit(1)) --nb;
+    while (nb > 2 && tma_smem<FD, TIN, TOUT, STAGE>(nb) > tma_smem_limit(1)) --nb;
     return nb;
 }
 
@@ -848,8 +855,8 @@ static cudaError_t launch_one(const StageMaps &m, const StageArgs &a, int *err, 
         }
         if (tma_minb_fd_env() == 2) {
             const int lim = tma_smem_limit(2);
-            if (tma_smem<TIN, TOUT, STAGE>(4) <= lim) return LNB(4, 2);
-            if (tma_smem<TIN, TOUT, STAGE>(3) <= lim) return LNB(3, 2);
+            if (tma_smem<SCHEME, TIN, TOUT, STAGE>(4) <= lim) return LNB(4, 2);
+            if (tma_smem<SCHEME, TIN, TOUT, STAGE>(3) <= lim) return LNB(3, 2);
             return LNB(2, 2);
         }
         switch (tma_fd_ring<TIN, TOUT, STAGE>()) {
@@ -867,8 +874,8 @@ static cudaError_t launch_one(const StageMaps &m, const StageArgs &a, int *err, 
         }
         if (tma_minb_env() == 1) return LNB(4, 1);
         const int lim = tma_smem_limit(2);
-        if (tma_smem<TIN, TOUT, STAGE>(4) <= lim) return LNB(4, 2);
-        if (tma_smem<TIN, TOUT, STAGE>(3) <= lim) return LNB(3, 2);
+        if (tma_smem<SCHEME, TIN, TOUT, STAGE>(4) <= lim) return LNB(4, 2);
+        if (tma_smem<SCHEME, TIN, TOUT, STAGE>(3) <= lim) return LNB(3, 2);
         return LNB(2, 2);
     }
 #undef LNB

@@ -60,7 +60,7 @@ struct cosenu_batch {
 
 namespace {
 
-constexpr int NMAP_B = 7;  // tensor maps per member (the TMA kernel's NMAP)
+constexpr int NMAP_B = 8;  // tensor maps per member (the TMA kernel's NMAP)
 
 int bfail(cosenu_batch *b, int code, const std::string &msg)
 {
@@ -308,7 +308,8 @@ int cosenu_batch_create(int n, const cosenu_params *params, cosenu_batch **out)
         return bail(COSENU_ERR_NOMEM);
     // per parity and member, in the order of the TMA kernel's MapIdx.  FP64:
     // Y, U0, U1 input boxes (with halo), Y, A, U0 tiles.  FP32-bulk: the
-    // current Y, D1, D2 input boxes, the D2 tile, -, the D1 tile, the D3 box.
+    // current Y, D1, D2 input boxes, the D2 tile, -, the D1 tile, the D3 box,
+    // the current Y in stage 4's rows.
     std::vector<CUtensorMap> maps(2 * NMAP_B * (size_t)n);
     for (int par = 0; par < 2; ++par)
         for (int i = 0; i < n; ++i) {
@@ -321,6 +322,7 @@ int cosenu_batch_create(int n, const cosenu_params *params, cosenu_batch **out)
             mp[4] = c->mA32;
             mp[5] = c->mU0_32;
             mp[6] = c->mU2_40;
+            mp[7] = c->mYb40s4[b->fp32 ? par : 0];
         }
     cudaMemcpyAsync(b->d_maps, maps.data(), maps.size() * sizeof(CUtensorMap),
                     cudaMemcpyHostToDevice, b->stream);

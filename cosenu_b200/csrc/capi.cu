@@ -200,9 +200,10 @@ cudaError_t launch_stage(cosenu_ctx *ctx, int stage, cudaStream_t s)
             mB = &ctx->mY32;  // unused
         } else {
             // input Y + D with the halo; stage 4 also reads D1, D2 at its own cells
-            mY = &ctx->mYb40[ctx->ypar];
-            mX = stage == 1 ? mY : (stage == 2 ? &ctx->mU0_40 : (stage == 3 ? &ctx->mU1_40
-                                                                             : &ctx->mU2_40));
+            mY = stage == 4 ? &ctx->mYb40s4[ctx->ypar] : &ctx->mYb40[ctx->ypar];
+            mX = stage == 1 ? &ctx->mYb40[ctx->ypar]
+                            : (stage == 2 ? &ctx->mU0_40 : (stage == 3 ? &ctx->mU1_40
+                                                                       : &ctx->mU2_40));
             mA = &ctx->mU0_32;
             mB = &ctx->mU1_32;
         }
@@ -482,20 +483,25 @@ int ctx_create(const cosenu_params *pp, cosenu_ctx **out, int layout)
     }
     cudaMemsetAsync(ctx->err_flag, 0, 64, ctx->stream);
     if (ctx->use_tma) {
+        // box rows follow the row count of the stages that read each map (the TMA
+        // kernel's rows(): 12 for the latency-bound FD stages, else 8)
         const int ub = ctx->fp32 ? 4 : 8, bx = tma_box_x(8), bxu = tma_box_x(ub),
-                  bt = tma_box_tile(), br = tma_box_rows(p.scheme);
-        int r = make_state_map(&ctx->mYb40[0], ctx->Yb[0], 8, ctx->ld, p.nvz, ctx->cs, bx, br);
-        if (!r) r = make_state_map(&ctx->mYb40[1], ctx->Yb[1], 8, ctx->ld, p.nvz, ctx->cs, bx, br);
-        if (!r) r = make_state_map(&ctx->mU0_40, ctx->U0, ub, ctx->ld, p.nvz, ctx->cs, bxu, br);
+                  bt = tma_box_tile(), rw = tma_box_rows(p.scheme, true),
+                  rn = tma_box_rows(p.scheme, false), ru = ctx->fp32 ? rw : rn;
+        int r = make_state_map(&ctx->mYb40[0], ctx->Yb[0], 8, ctx->ld, p.nvz, ctx->cs, bx, rw);
+        if (!r) r = make_state_map(&ctx->mYb40[1], ctx->Yb[1], 8, ctx->ld, p.nvz, ctx->cs, bx, rw);
+        if (!r) r = make_state_map(&ctx->mYb40s4[0], ctx->Yb[0], 8, ctx->ld, p.nvz, ctx->cs, bx, rn);
+        if (!r) r = make_state_map(&ctx->mYb40s4[1], ctx->Yb[1], 8, ctx->ld, p.nvz, ctx->cs, bx, rn);
+        if (!r) r = make_state_map(&ctx->mU0_40, ctx->U0, ub, ctx->ld, p.nvz, ctx->cs, bxu, ru);
         // (FP64 stage 3 reads U1 in 40-cell rows, see the TMA kernel's Layout)
         if (!r) r = make_state_map(&ctx->mU1_40, ctx->U1, ub, ctx->ld, p.nvz, ctx->cs,
-                                   ctx->fp32 ? bxu : bt + 8, br);
-        if (!r) r = make_state_map(&ctx->mY32, ctx->Yb[0], 8, ctx->ld, p.nvz, ctx->cs, bt, br);
-        if (!r) r = make_state_map(&ctx->mA32, ctx->Yb[1], 8, ctx->ld, p.nvz, ctx->cs, bt, br);
-        if (!r) r = make_state_map(&ctx->mU0_32, ctx->U0, ub, ctx->ld, p.nvz, ctx->cs, bt, br);
-        if (!r) r = make_state_map(&ctx->mU1_32, ctx->U1, ub, ctx->ld, p.nvz, ctx->cs, bt, br);
+                                   ctx->fp32 ? bxu : bt + 8, ru);
+        if (!r) r = make_state_map(&ctx->mY32, ctx->Yb[0], 8, ctx->ld, p.nvz, ctx->cs, bt, rn);
+        if (!r) r = make_state_map(&ctx->mA32, ctx->Yb[1], 8, ctx->ld, p.nvz, ctx->cs, bt, rn);
+        if (!r) r = make_state_map(&ctx->mU0_32, ctx->U0, ub, ctx->ld, p.nvz, ctx->cs, bt, rn);
+        if (!r) r = make_state_map(&ctx->mU1_32, ctx->U1, ub, ctx->ld, p.nvz, ctx->cs, bt, rn);
         if (!r && ctx->U2)
-            r = make_state_map(&ctx->mU2_40, ctx->U2, ub, ctx->ld, p.nvz, ctx->cs, bxu, br);
+            r = make_state_map(&ctx->mU2_40, ctx->U2, ub, ctx->ld, p.nvz, ctx->cs, bxu, rn);
         if (!ctx->U2) ctx->mU2_40 = ctx->mU1_40;  // unused in FP64
         if (!r && tma_prepare() != cudaSuccess) r = -2;
         if (r) {

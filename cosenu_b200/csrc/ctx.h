@@ -19,7 +19,7 @@ cudaError_t launch_moments(const double *X, double *M, const double *vz, long lo
                            int nz, int nvz, int tz, int tv, cudaStream_t s);
 int make_state_map(CUtensorMap *map, const void *base, int elem_bytes, int ld, int nvz,
                    long long cs, int box_cells, int box_rows);
-int tma_box_rows(int scheme);
+int tma_box_rows(int scheme, bool wide);
 int tma_box_x(int elem_bytes);
 int tma_box_tile();
 int tma_max_nvz();
@@ -64,6 +64,7 @@ struct cosenu_ctx {
     bool use_tma = false;
     int nsm = 148;
     CUtensorMap mYb40[2], mU0_40, mU1_40, mU2_40, mY32, mA32, mU0_32, mU1_32;
+    CUtensorMap mYb40s4[2];  // FP32-bulk stage 4's view of Yb (its own row count)
     int *err_flag = nullptr;  // device word set by bounded waits that expired
     unsigned long long wait_ns = 2000000000ull;  // limit of each pipeline wait
     int stall = 0;            // test hook: TMA producers issue no copies

@@ -51,12 +51,17 @@ constexpr int HALO = 4;          // cells each side in the input box
 // 0, 20, 8, 28, ... for components 0..7; 44 floats = 44 words: 0, 12, 24, ...).
 template <class T> constexpr int xw() { return sizeof(T) == 8 ? 42 : 44; }
 // v rows per chunk = consumer warps.  FV runs two blocks per SM (<= 96
-// registers per thread) with 8; FD, one block per SM bound by latency more than
-// by its FP64 work, runs 12 (still ~160 registers per thread) to hide it.
-template <int SCHEME> constexpr int rows() { return SCHEME == FV ? 8 : 12; }
-template <int SCHEME> constexpr int nthr() { return rows<SCHEME>() * 32 + 32; }  // + producer
+// registers per thread) with 8.  FD runs one block per SM: the stages that move
+// few bytes per cell (FP64 stage 1, FP32-bulk stages 1-3) are bound by latency
+// and run 12 (13 warps, ~126 registers, no spills: 0.230 -> 0.205 ms for FP64
+// stage 1 at nz 32768 x nvz 256); the HBM-bound stages keep 8, whose smaller
+// chunks keep fewer bytes in flight (12 rows: FP64 stage 3 0.436 -> 0.490 ms).
+template <int SCHEME, int STAGE, bool INC> constexpr int rows()
+{
+    return (SCHEME == FD && ((!INC && STAGE == 1) || (INC && STAGE <= 3))) ? 12 : 8;
+}
 // tensor maps per ensemble member (MapIdx lists them)
-constexpr int NMAP = 7;
+constexpr int NMAP = 8;
 #define TMA_MAX_NVZ 1024
 
 __device__ __forceinline__ uint32_t smem_u32(const void *p)
@@ -162,8 +167,9 @@ template <int NCONS> __device__ __forceinline__ void consumer_sync()
 // (the tensor maps put components before rows): the input box X, then Y, then
 // the own-cell tiles A (and B).
 template <int SCHEME, class TIN, class TOUT, int STAGE> struct Layout {
-    static constexpr int R = rows<SCHEME>();
     static constexpr bool INC = inc_form<TIN, TOUT>();
+    static constexpr int R = rows<SCHEME, STAGE, INC>();
+    static constexpr int NTHR = R * 32 + 32;  // consumer warps + producer warp
     // FP64 stage 3 streams the most bytes per chunk: its 40-cell rows keep a
     // two-buffer ring within half an SM's shared memory (two blocks per SM)
     static constexpr int XW = (!INC && STAGE == 3) ? TZ + 2 * HALO : xw<TIN>();
@@ -182,10 +188,11 @@ template <int SCHEME, class TIN, class TOUT, int STAGE> struct Layout {
 
 // Index of each operand's tensor map among a member's NMAP maps (ensembles).
 // FP64:      0 Y (halo box), 1 U0 (halo), 2 U1 (halo), 3 Y (tile), 4 A (tile), 5 U0 (tile)
-// FP32-bulk: 0 current Y (halo), 1 D1 (halo), 2 D2 (halo), 3 D2 (tile), 5 D1 (tile), 6 D3 (halo)
+// FP32-bulk: 0 current Y (halo), 1 D1 (halo), 2 D2 (halo), 3 D2 (tile), 5 D1 (tile), 6 D3 (halo),
+//            7 current Y (halo) in the row count of stage 4
 template <bool INC, int STAGE> struct MapIdx {
     static constexpr int X = STAGE == 1 ? 0 : (STAGE == 3 ? 2 : (INC && STAGE == 4 ? 6 : 1));
-    static constexpr int Y = INC ? 0 : 3;
+    static constexpr int Y = INC ? (STAGE == 4 ? 7 : 0) : 3;
     static constexpr int A = INC ? 5 : (STAGE == 3 ? 5 : 4);
     static constexpr int B = 3;
 };
@@ -232,7 +239,7 @@ __device__ __forceinline__ void row_values(double v0, double dv, double dz, int 
 // right-hand side is evaluated in FP64 in both forms, except the FP32-bulk
 // WENO7 weights and candidates (FP32 on FP64 stencil differences).
 template <int SCHEME, bool GEN, int STAGE, class TIN, class TOUT, int NBUF, bool BATCHED, int MINB>
-__global__ void __launch_bounds__(tma::nthr<SCHEME>(), MINB)
+__global__ void __launch_bounds__(tma::Layout<SCHEME, TIN, TOUT, STAGE>::NTHR, MINB)
     rk4_stage_tma_kernel(const __grid_constant__ CUtensorMap mX,
                          const __grid_constant__ CUtensorMap mY,
                          const __grid_constant__ CUtensorMap mA,
@@ -727,7 +734,8 @@ int make_state_map(CUtensorMap *map, const void *base, int elem_bytes, int ld, i
 
 int tma_box_x(int elem_bytes) { return elem_bytes == 8 ? tma::xw<double>() : tma::xw<float>(); }
 int tma_box_tile() { return tma::TZ; }
-int tma_box_rows(int scheme) { return scheme == FV ? tma::rows<FV>() : tma::rows<FD>(); }
+// Rows of a map's box: `wide` for the operands of the 12-row FD stages.
+int tma_box_rows(int scheme, bool wide) { return scheme == FD && wide ? 12 : 8; }
 // largest nvz the TMA layout is offered for (the range its tests cover; the
 // kernel itself keeps no per-row state in shared memory)
 int tma_max_nvz() { return TMA_MAX_NVZ; }
@@ -773,7 +781,7 @@ static cudaError_t launch_nb(const StageMaps &m, const StageArgs &a, int *err, i
         return cudaSuccess;
     }
     const int shmem = tma_smem<SCHEME, TIN, TOUT, STAGE>(NB);
-    constexpr int NT = tma::nthr<SCHEME>();
+    constexpr int NT = tma::Layout<SCHEME, TIN, TOUT, STAGE>::NTHR;
     if (bd)
         kernb<<<nblocks, NT, shmem, s>>>(*m.x, *m.y, *m.a, *m.b, a, err, *bd);
     else

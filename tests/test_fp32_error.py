@@ -82,3 +82,16 @@ def test_fp32_bulk_benchmark_grid_against_reference(gpu_lib):
             got = _i(case, sim.download())
             err = maxabs_per_comp(got[:, :, cols], d[f"rho_{t}_columns"])
             assert np.all(err <= 1e-12), (t, err)
+
+
+def test_fp32_bulk_large_fv_grid_against_reference(gpu_lib):
+    """The FV grid of the FP32-bulk workload (nz 65536 x nvz 512), 5 steps,
+    against the reference's own dump: <= 1e-11 per component."""
+    case, d = load_golden("c3_ref")
+    cols = d["columns"]
+    with gpu_from_case(case, precision="fp32") as sim:
+        sim.init_seeded(int(d["seed"]))
+        sim.evolve(5)
+        got = _i(case, sim.download())
+    err = maxabs_per_comp(got[:, :, cols], d["rho_5_columns"])
+    assert np.all(err <= 1e-11), err

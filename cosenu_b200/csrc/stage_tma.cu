@@ -790,11 +790,11 @@ static cudaError_t launch_nb(const StageMaps &m, const StageArgs &a, int *err, i
 }
 
 // Ring depth of the FD kernel (one block per SM): the deepest ring of at most
-// 4 buffers that total at most ~112 KB.  Measured at nz 32768 x nvz 256, more
-// bytes in flight per SM lower the achieved HBM bandwidth (FP64 stages 2-3,
-// 53 KB per chunk: 0.441 / 0.534 / 0.545 ms per stage with 2 / 3 / 4 buffers;
-// FP64 stage 4, 37 KB: 3 buffers best; FP64 stage 1, 20 KB: 4 buffers
-// 0.318 ms, 5 buffers 0.344 ms).
+// 4 buffers that total at most 144 KB.  Measured at nz 32768 x nvz 256:
+// stages of 53-54 KB chunks (FP64 stage 3) are fastest with 2 buffers
+// (0.441 / 0.534 / 0.545 ms with 2 / 3 / 4), FP64 stages 2 and 4 (38 KB) with
+// 3, the FP32-bulk stages (48 KB chunks) with 3 (stage 4: 0.358 ms with 2,
+// 0.320 ms with 3).
 // COSENU_TMA_RING=n (2..4) overrides the depth where it fits.
 static int tma_ring_env()
 {
@@ -811,7 +811,7 @@ static int tma_fd_ring()
 {
     using L = tma::Layout<FD, TIN, TOUT, STAGE>;
     int nb = 2;
-    while (nb < 4 && (nb + 1) * L::BUF <= 112 * 1024) ++nb;
+    while (nb < 4 && (nb + 1) * L::BUF <= 144 * 1024) ++nb;
     const int e = tma_ring_env();
     if (e) nb = e;
     while (nb > 2 && tma_smem<FD, TIN, TOUT, STAGE>(nb) > tma_smem_limit(1)) --nb;

@@ -184,6 +184,12 @@ template <int SCHEME, class TIN, class TOUT, int STAGE> struct Layout {
     static constexpr int AB = INC ? (STAGE == 4 ? 2 * NCOMP * R * TZ * 4 : 0)
                                   : (STAGE >= 3 ? NCOMP * R * TZ * 8 : 0);
     static constexpr int BUF = ((XB + YB + AB) + 127) / 128 * 128;
+    // FV (two blocks per SM, <= 96 registers): each consumer warp accumulates
+    // the output moments of its rows in shared memory rather than in 12
+    // registers, where half an SM leaves room (all but FP64 stage 3); the
+    // other kernels keep them in registers and pair warps at the tile's end
+    static constexpr bool MSM = SCHEME == FV && (INC || STAGE != 3);
+    static constexpr int NRED = MSM ? R : R / 2;  // moment slots in shared memory
 };
 
 // Index of each operand's tensor map among a member's NMAP maps (ensembles).
@@ -256,8 +262,8 @@ __global__ void __launch_bounds__(tma::Layout<SCHEME, TIN, TOUT, STAGE>::NTHR, M
     uint64_t *full = reinterpret_cast<uint64_t *>(smem + NBUF * L::BUF);
     uint64_t *empty = full + NBUF;
     double(*s_mom)[TZ] = reinterpret_cast<double(*)[TZ]>(empty + NBUF);  // [6][TZ]
-    double(*s_red)[NMOM][TZ] = reinterpret_cast<double(*)[NMOM][TZ]>(s_mom + NMOM);  // [R/2]
-    StageArgs *s_args = reinterpret_cast<StageArgs *>(s_red + R / 2);  // batched: current member
+    double(*s_red)[NMOM][TZ] = reinterpret_cast<double(*)[NMOM][TZ]>(s_mom + NMOM);  // [NRED]
+    StageArgs *s_args = reinterpret_cast<StageArgs *>(s_red + L::NRED);  // batched: current member
 
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const int nzt = BATCHED ? bd.ntiles : a0.nz / TZ;
@@ -388,6 +394,11 @@ __global__ void __launch_bounds__(tma::Layout<SCHEME, TIN, TOUT, STAGE>::NTHR, M
                 mnext = an.Min[(long long)(tid / TZ) * an.nz + zn * TZ + tid % TZ];
         }
         double macc[NMOM] = {0, 0, 0, 0, 0, 0};
+        if constexpr (L::MSM) {
+            // this warp's moment slots (the previous tile's epilogue has read them)
+#pragma unroll
+            for (int m = 0; m < NMOM; ++m) s_red[warp][m][lane] = 0.0;
+        }
 
         for (int ch = 0; ch < nch; ++ch, ++it) {
             const int b = it % NBUF;
@@ -653,18 +664,38 @@ __global__ void __launch_bounds__(tma::Layout<SCHEME, TIN, TOUT, STAGE>::NTHR, M
                     const double Am = um[EXI] + um[BEXI];
                     const double Bm = um[EXR] - um[BEXR];
                     const double Cm = um[EE] - um[XX] - um[BEE] + um[BXX];
-                    macc[0] += Am;
-                    macc[1] += Bm;
-                    macc[2] += Cm;
-                    macc[3] += vzv * Am;
-                    macc[4] += vzv * Bm;
-                    macc[5] += vzv * Cm;
+                    if constexpr (L::MSM) {
+                        s_red[warp][0][lane] += Am;
+                        s_red[warp][1][lane] += Bm;
+                        s_red[warp][2][lane] += Cm;
+                        s_red[warp][3][lane] += vzv * Am;
+                        s_red[warp][4][lane] += vzv * Bm;
+                        s_red[warp][5][lane] += vzv * Cm;
+                    } else {
+                        macc[0] += Am;
+                        macc[1] += Bm;
+                        macc[2] += Cm;
+                        macc[3] += vzv * Am;
+                        macc[4] += vzv * Bm;
+                        macc[5] += vzv * Cm;
+                    }
                 }
             }
         }
         // tile epilogue: output moments (fixed-order sum over warps) and the
         // next tile's input moments
-        if (coll || BATCHED) {
+        if ((coll || BATCHED) && L::MSM) {
+            consumer_sync();
+            if (tid < NMOM * TZ) {
+                const int m = tid / TZ, zz = tid % TZ;
+                double s = 0.0;
+#pragma unroll
+                for (int w = 0; w < R; ++w) s += s_red[w][m][zz];
+                if (coll) a.Mout[(long long)m * a.nz + z0 + zz] = s;
+                s_mom[m][zz] = mnext;  // every consumer read this tile's values above
+            }
+            consumer_sync();
+        } else if (coll || BATCHED) {
             // warps w and w + R/2 pair up, then the R/2 pair sums are added
             // in a fixed order
             if (warp >= R / 2) {
@@ -748,7 +779,7 @@ template <int SCHEME, class TIN, class TOUT, int STAGE>
 static int tma_smem(int NB)
 {
     using L = tma::Layout<SCHEME, TIN, TOUT, STAGE>;
-    return NB * L::BUF + 2 * NB * 8 + (1 + L::R / 2) * NMOM * tma::TZ * 8 +
+    return NB * L::BUF + 2 * NB * 8 + (1 + L::NRED) * NMOM * tma::TZ * 8 +
            (int)sizeof(StageArgs);
 }
 

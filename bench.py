@@ -604,8 +604,9 @@ def run_fp32_study(args):
 
 
 def run_surrogate(args):
-    """The surrogate workload (nz fixed at 512 to fit the training set in
-    the run time): solver targets for a training and a
+    """The surrogate workload (nz fixed at 512 by default to fit the training
+    set in the run time; --sur-nz 0 draws it log-uniform in [512, 8192] as
+    the ensemble distribution does): solver targets for a training and a
     held-out set, a committee of networks trained on the GPU, held-out error
     against the solver with and without the disagreement fallback, and the
     time of both routes."""
@@ -616,8 +617,9 @@ def run_surrogate(args):
                                        surrogate_instances)
 
     torch.cuda.set_device(0)
-    train = surrogate_instances(args.train, seed=21, nz=args.sur_nz, t_factor=args.t_factor)
-    test = surrogate_instances(args.test, seed=22, nz=args.sur_nz, t_factor=args.t_factor)
+    sur_nz = args.sur_nz or None  # 0: log-uniform in [512, 8192]
+    train = surrogate_instances(args.train, seed=21, nz=sur_nz, t_factor=args.t_factor)
+    test = surrogate_instances(args.test, seed=22, nz=sur_nz, t_factor=args.t_factor)
     t0 = time.perf_counter()
     y_train = solve_pee(train)
     t_train_data = time.perf_counter() - t0
@@ -680,7 +682,7 @@ def run_surrogate(args):
     tot = lambda d: sum(d.values())  # noqa: E731
     print(json.dumps({
         "metric": "surrogate vs solver on held-out instances", "train": len(train),
-        "test": len(test), "nz": args.sur_nz, "nvz": 128, "t_factor": args.t_factor,
+        "test": len(test), "nz": args.sur_nz or "log-uniform [512, 8192]", "nvz": 128, "t_factor": args.t_factor,
         "mean_abs_err": float(err.mean()), "rms_err": float(np.sqrt((err ** 2).mean())),
         "p95_instance_max_err": float(np.percentile(err.max(axis=1), 95)),
         "fallback_threshold": args.threshold, "fallback_fraction": float(fb.mean()),
@@ -701,6 +703,74 @@ def run_surrogate(args):
         "held_out_nz_loguniform": gen,
     }), flush=True)
     sur.close()
+
+
+def run_surrogate_gemm_study(args):
+    """Device time of the surrogate network's kernels with each GEMM kernel
+    (tcgen05 with the accumulator in tensor memory, and the warp-level
+    mma.sync kernel, COSENU_MLP_GEMM=mma): a committee of 4 networks
+    258 -> 3 x 512 -> 128 on synthetic features and targets of the workload's
+    shapes; one training epoch over 4096 rows (batches of 64) and one
+    committee inference over 2048 rows, CUDA events around every launch."""
+    import numpy as np
+    import torch
+
+    from cosenu_b200.surrogate import Surrogate
+
+    torch.cuda.set_device(0)
+    rng = np.random.default_rng(5)
+    x_train = rng.normal(size=(4096, 258)).astype(np.float32)
+    y_train = rng.uniform(0.2, 1.0, (4096, 128)).astype(np.float32)
+    x_test = rng.normal(size=(2048, 258)).astype(np.float32)
+    widths = [(272, 512), (512, 512), (512, 512), (512, 128)]  # input padded to 272
+    flop_fwd_row = 2 * sum(a * b for a, b in widths)
+    out = {}
+    prev = os.environ.get("COSENU_MLP_GEMM")
+    try:
+        for gemm in ("tcgen05", "mma"):
+            os.environ["COSENU_MLP_GEMM"] = gemm
+            sur = Surrogate(n_models=4)
+            sur.fit(x_train, y_train, epochs=2, batch=64, lr=1e-4)  # warm-up, buffers sized
+            sur.committee(x_test)
+            sur.set_timing(True)
+            for k, m in enumerate(sur.models):
+                m.train(epochs=1, batch=64, lr=1e-5, seed=7000 + k)
+            train_ms = sur.timing()
+            sur.set_timing(True)
+            mean, _ = sur.committee(x_test)
+            infer_ms = sur.timing()
+            sur.set_timing(False)
+            t0 = time.perf_counter()
+            sur.committee(x_test)
+            wall = time.perf_counter() - t0
+            flops = 4 * flop_fwd_row * x_test.shape[0]
+            out[gemm] = {"training_one_epoch_committee_ms": train_ms,
+                         "inference_committee_ms": infer_ms,
+                         "inference_gemm_tflops": flops / (infer_ms["gemm"] * 1e-3) / 1e12,
+                         "inference_wall_s": wall, "pred": mean}
+            sur.close()
+    finally:
+        if prev is None:
+            os.environ.pop("COSENU_MLP_GEMM", None)
+        else:
+            os.environ["COSENU_MLP_GEMM"] = prev
+    diff = float(np.abs(out["tcgen05"].pop("pred") - out["mma"].pop("pred")).max())
+    try:
+        bf16_peak = float(json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))["bf16_tflops"])
+    except Exception:
+        bf16_peak = 1590.0  # fallback
+    print(json.dumps({
+        "metric": "surrogate network device time by GEMM kernel",
+        "network": "258 -> 3 x 512 (GELU) -> 128, BF16 operands, FP32 accumulate, committee of 4",
+        "data": "synthetic features / targets", "training_rows": 4096, "batch": 64,
+        "inference_rows": 2048, **out,
+        "gemm_speedup_inference": out["mma"]["inference_committee_ms"]["gemm"] /
+        out["tcgen05"]["inference_committee_ms"]["gemm"],
+        "gemm_speedup_training": out["mma"]["training_one_epoch_committee_ms"]["gemm"] /
+        out["tcgen05"]["training_one_epoch_committee_ms"]["gemm"],
+        "bf16_peak_tflops": bf16_peak,
+        "max_abs_diff_committee_mean": diff,
+    }), flush=True)
 
 
 def run_snapshot_study(args):
@@ -778,9 +848,12 @@ def main():
     ap.add_argument("--instances", type=int, default=256, help="c4: ensemble size")
     ap.add_argument("--train", type=int, default=4096, help="c5: training instances")
     ap.add_argument("--test", type=int, default=512, help="c5: held-out instances")
-    ap.add_argument("--sur-nz", type=int, default=512, help="c5: nz of the solver runs")
+    ap.add_argument("--sur-nz", type=int, default=512,
+                    help="c5: nz of the solver runs (0: log-uniform in [512, 8192])")
     ap.add_argument("--epochs", type=int, default=300, help="c5: training epochs")
     ap.add_argument("--threshold", type=float, default=1e-2, help="c5: fallback threshold")
+    ap.add_argument("--gemm-study", action="store_true",
+                    help="c5: device time of the network with each GEMM kernel")
     ap.add_argument("--gen-test", type=int, default=64,
                     help="c5: held-out instances with nz log-uniform in [512, 8192]")
     ap.add_argument("--fp32-study", action="store_true",
@@ -809,7 +882,10 @@ def main():
             run_ensemble(args)
         return
     if args.workload == "c5":
-        run_surrogate(args)
+        if args.gemm_study:
+            run_surrogate_gemm_study(args)
+        else:
+            run_surrogate(args)
         return
     WORKLOAD.clear()
     WORKLOAD.update(WORKLOADS[args.workload])

@@ -3,20 +3,28 @@
 // of a simulation to its late-time, angle-resolved survival probability.
 // BF16 weights and activations feed the tensor cores with FP32 accumulation;
 // FP32 master weights are updated by AdamW.  Everything here is hand written:
-// the GEMMs (mma.sync m16n8k16 BF16 tiles; the layers are a few hundred wide,
-// so each GEMM is small and latency bound), the GELU forward/backward, the
-// loss, the bias reductions and the optimizer.
+// the GEMMs (tcgen05.mma with the accumulator in tensor memory, mlp_gemm.cu;
+// the warp-level mma.sync m16n8k16 kernel below stays for operands that do
+// not fit that path and as the comparison the surrogate timing reports with
+// COSENU_MLP_GEMM=mma), the GELU forward/backward, the loss, the bias
+// reductions and the optimizer.
 //
 // Layout: activations are batch-major rows; layer l has W_l [out][in] and b_l
 // [out]; the input width is padded to a multiple of 16 with zero columns.
 #include <cuda_bf16.h>
 
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
 #include <string>
 #include <vector>
 
 #include "../../include/cosenu_b200.h"
+
+cudaError_t mlp_gemm_tc(const __nv_bfloat16 *A, long long sam, long long sak,
+                        const __nv_bfloat16 *B, long long sbk, long long sbn, int M, int N, int K,
+                        float *C, int ldc, const float *bias, __nv_bfloat16 *H, int ldh, int act,
+                        int *err, cudaStream_t s);
 
 namespace {
 
@@ -120,10 +128,15 @@ __global__ void __launch_bounds__(128) gemm_bf16_kernel(
             }
 }
 
+// tcgen05 path when `tc` and the operands fit it; a launch error stays
+// pending for the caller's next cudaGetLastError.
 void gemm(const __nv_bfloat16 *A, long long sam, long long sak, const __nv_bfloat16 *B,
           long long sbk, long long sbn, int M, int N, int K, float *C, int ldc, const float *bias,
-          __nv_bfloat16 *H, int ldh, int act, cudaStream_t s)
+          __nv_bfloat16 *H, int ldh, int act, bool tc, int *err, cudaStream_t s)
 {
+    if (tc && mlp_gemm_tc(A, sam, sak, B, sbk, sbn, M, N, K, C, ldc, bias, H, ldh, act, err, s) !=
+                  cudaErrorNotSupported)
+        return;
     dim3 grid((N + GT - 1) / GT, (M + GT - 1) / GT);
     gemm_bf16_kernel<<<grid, 128, 0, s>>>(A, sam, sak, B, sbk, sbn, M, N, K, C, ldc, bias, H, ldh,
                                           act);
@@ -247,6 +260,8 @@ struct cosenu_mlp {
     int ndata = 0;
     long long t_step = 0;
     cudaStream_t stream = nullptr;
+    bool tc = true;        // GEMMs on tcgen05 (COSENU_MLP_GEMM=mma: the mma.sync kernel)
+    int *derr = nullptr;   // error word of the tcgen05 GEMM's bounded waits
     // host inputs of forward / loss_grad staged here (grown on demand)
     float *dxin = nullptr, *dtin = nullptr;
     size_t xin_cap = 0, tin_cap = 0;
@@ -323,6 +338,20 @@ int mfail(cosenu_mlp *n, int code, const std::string &msg)
             return mfail(net, COSENU_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); \
     } while (0)
 
+// After a synchronisation of the stream: a pending launch error, or an
+// expired wait recorded by the tcgen05 GEMM (the word is cleared).
+int check_device(cosenu_mlp *net)
+{
+    MCK(cudaGetLastError());
+    int h = 0;
+    MCK(cudaMemcpy(&h, net->derr, sizeof(int), cudaMemcpyDeviceToHost));
+    if (h) {
+        MCK(cudaMemset(net->derr, 0, sizeof(int)));
+        return mfail(net, COSENU_ERR_CUDA, "tensor-core GEMM: a pipeline wait timed out");
+    }
+    return COSENU_OK;
+}
+
 // Host rows (and targets) copied into the staging buffers, grown on demand.
 int stage_inputs(cosenu_mlp *net, const float *x_host, const float *t_host, int rows)
 {
@@ -381,7 +410,7 @@ void forward(cosenu_mlp *net, int rows)
         Timed tm(net, K_GEMM);
         gemm(x, kin, 1, net->wb + net->woff[l], 1, kin, rows, net->dout[l], kin, net->Z[l],
              net->dout[l], net->w + net->boff[l], last ? nullptr : net->Hb[l], net->dout[l],
-             last ? 0 : 1, net->stream);
+             last ? 0 : 1, net->tc, net->derr, net->stream);
         x = net->Hb[l];
         kin = net->dout[l];
     }
@@ -406,7 +435,7 @@ void backward(cosenu_mlp *net, int rows, int nblk_loss)
         {
             Timed tm(net, K_GEMM);
             gemm(net->dAb, 1, dout, xin, din, 1, dout, din, rows, net->g + net->woff[l], din,
-                 nullptr, nullptr, 0, 0, net->stream);
+                 nullptr, nullptr, 0, 0, net->tc, net->derr, net->stream);
         }
         {
             Timed tm(net, K_ELEM);
@@ -418,7 +447,7 @@ void backward(cosenu_mlp *net, int rows, int nblk_loss)
             {
                 Timed tm(net, K_GEMM);
                 gemm(net->dAb, dout, 1, net->wb + net->woff[l], din, 1, rows, din, dout, net->dB,
-                     din, nullptr, nullptr, 0, 0, net->stream);
+                     din, nullptr, nullptr, 0, 0, net->tc, net->derr, net->stream);
             }
             int n = rows * din;
             Timed tm(net, K_ELEM);
@@ -480,11 +509,15 @@ int cosenu_mlp_create(int n_in, int n_hidden, int n_hidden_layers, int n_out, ui
         cudaMalloc(&net->m1, net->nparam * 4) != cudaSuccess ||
         cudaMalloc(&net->m2, net->nparam * 4) != cudaSuccess ||
         cudaMalloc(&net->wb, net->nparam * 2) != cudaSuccess ||
-        cudaMalloc(&net->partial, 1024 * 4 + 8) != cudaSuccess) {
+        cudaMalloc(&net->partial, 1024 * 4 + 8) != cudaSuccess ||
+        cudaMalloc(&net->derr, sizeof(int)) != cudaSuccess ||
+        cudaMemset(net->derr, 0, sizeof(int)) != cudaSuccess) {
         cosenu_mlp_destroy(net);
         return COSENU_ERR_NOMEM;
     }
     net->eacc = reinterpret_cast<double *>(net->partial + 1024);
+    const char *gk = std::getenv("COSENU_MLP_GEMM");
+    net->tc = !(gk && std::strcmp(gk, "mma") == 0);
     *out = net;
     return cosenu_mlp_set_params(net, h.data());
 }
@@ -494,7 +527,8 @@ int cosenu_mlp_destroy(cosenu_mlp *net)
     if (!net) return COSENU_OK;
     if (net->stream) cudaStreamSynchronize(net->stream);
     void *bufs[] = {net->w, net->g, net->m1, net->m2, net->wb, net->partial, net->xb, net->dA,
-                    net->dB, net->dAb, net->T, net->dX, net->dT, net->didx, net->dxin, net->dtin};
+                    net->dB, net->dAb, net->T, net->dX, net->dT, net->didx, net->dxin, net->dtin,
+                    net->derr};
     for (void *b : bufs)
         if (b) cudaFree(b);
     for (auto p : net->Z)
@@ -557,7 +591,7 @@ int cosenu_mlp_forward(cosenu_mlp *net, const float *x_host, int rows, float *y_
                         cudaMemcpyDeviceToHost, net->stream));
     MCK(cudaStreamSynchronize(net->stream));
     collect_times(net);
-    return COSENU_OK;
+    return check_device(net);
 }
 
 // Mean-squared-error loss and its gradient with respect to the FP32 master
@@ -581,6 +615,7 @@ int cosenu_mlp_loss_grad(cosenu_mlp *net, const float *x_host, const float *t_ho
         MCK(cudaMemcpyAsync(grad_host, net->g, net->nparam * 4, cudaMemcpyDeviceToHost, net->stream));
     MCK(cudaStreamSynchronize(net->stream));
     collect_times(net);
+    if ((rc = check_device(net)) != COSENU_OK) return rc;
     double s = 0;
     for (float p : part) s += p;
     if (loss) *loss = (float)(s / ((double)rows * net->nout));
@@ -664,9 +699,9 @@ int cosenu_mlp_train(cosenu_mlp *net, int epochs, int batch, float lr, float wei
         MCK(cudaMemcpyAsync(&esum, net->eacc, sizeof(double), cudaMemcpyDeviceToHost, net->stream));
         MCK(cudaStreamSynchronize(net->stream));
         collect_times(net);
+        if ((rc = check_device(net)) != COSENU_OK) return rc;
         if (epoch_loss) epoch_loss[e] = (float)(esum / ecount);
     }
-    MCK(cudaGetLastError());
     return COSENU_OK;
 }
 

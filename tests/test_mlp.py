@@ -40,9 +40,15 @@ def _rel(a, b):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("shape", [(30, 32, 2, 16, 70), (258, 512, 3, 128, 64)])
-def test_gpu_forward_and_gradients_against_oracle(gpu_lib, shape):
+@pytest.mark.parametrize("gemm", ["tcgen05", "mma"])
+@pytest.mark.parametrize("shape", [(30, 32, 2, 16, 70), (258, 512, 3, 128, 64),
+                                   (258, 512, 3, 128, 1029)])
+def test_gpu_forward_and_gradients_against_oracle(gpu_lib, monkeypatch, shape, gemm):
+    """Both GEMM kernels: tcgen05 (the default) and the warp-level mma.sync
+    one (COSENU_MLP_GEMM=mma).  Widths below one 64-column tile, K below one
+    64-deep stage, and 1029 rows (nine 128-row tiles, the last ragged)."""
     from cosenu_b200.surrogate import MLP
+    monkeypatch.setenv("COSENU_MLP_GEMM", gemm)
     n_in, nh, nl, nout, rows = shape
     rng = np.random.default_rng(1)
     net = MLP(n_in, nh, nl, nout, seed=3)
@@ -106,3 +112,26 @@ def test_gpu_training_fits_smooth_map(gpu_lib):
     assert losses[-1] < losses[0]
     assert final < base / 20, (base, final)
     net.close()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("rows", [1, 127, 128, 129, 2053])
+def test_gpu_tcgen05_gemm_matches_mma_sync_kernel(gpu_lib, monkeypatch, rows):
+    """The same network evaluated with both GEMM kernels: forward outputs and
+    the gradient (forward, dW = dZ^T X with both operands transposed, dX =
+    dZ W with W transposed) agree to FP32 summation order and the odd BF16
+    rounding flip of an activation."""
+    from cosenu_b200.surrogate import MLP
+    rng = np.random.default_rng(rows)
+    x = rng.uniform(0, 1.5, (rows, 258)).astype(np.float32)
+    t = rng.uniform(0, 1, (rows, 128)).astype(np.float32)
+    out = {}
+    for gemm in ("tcgen05", "mma"):
+        monkeypatch.setenv("COSENU_MLP_GEMM", gemm)
+        net = MLP(258, 512, 3, 128, seed=11)
+        out[gemm] = (net.forward(x), net.loss_grad(x, t))
+        net.close()
+    (ya, (la, ga)), (yb, (lb, gb)) = out["tcgen05"], out["mma"]
+    assert _rel(ya, yb) <= 2e-3
+    assert abs(la - lb) <= 2e-3 * lb
+    assert _rel(ga, gb) <= 5e-3

@@ -263,7 +263,12 @@ int cosenu_batch_set_config(cosenu_batch *b, int use_tma, int tz, const int *tv_
  * weights and activations on the tensor cores with FP32 accumulation, FP32
  * master weights trained by AdamW on the mean-squared error.  Parameters are
  * one flat FP32 vector: for each layer W [out][in] (in padded to a multiple
- * of 16, padding columns zero) then b [out]. */
+ * of 16, padding columns zero) then b [out].  n_hidden must be a multiple of
+ * 16 and n_out of 8.  The GEMMs run on tcgen05 (tensor-memory accumulator);
+ * with the environment variable COSENU_MLP_GEMM=mma at cosenu_mlp_create the
+ * net uses the warp-level mma.sync kernel instead (the same sums in the same
+ * order, kept for comparison).  A GEMM whose bounded internal wait expires
+ * makes the next synchronising call return COSENU_ERR_CUDA. */
 typedef struct cosenu_mlp cosenu_mlp;
 int cosenu_mlp_create(int n_in, int n_hidden, int n_hidden_layers, int n_out, uint64_t seed,
                       int device, cosenu_mlp **out);

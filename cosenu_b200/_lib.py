@@ -23,7 +23,8 @@ EXPORTS = (
     "cosenu_params_default", "cosenu_create", "cosenu_destroy", "cosenu_last_error",
     "cosenu_set_vac_pars", "cosenu_set_collective_pars", "cosenu_set_stream", "cosenu_grid",
     "cosenu_upload", "cosenu_download", "cosenu_set_profile", "cosenu_set_state0",
-    "cosenu_mark_state0", "cosenu_step", "cosenu_step_stage", "cosenu_synchronize",
+    "cosenu_mark_state0", "cosenu_step", "cosenu_step_stage", "cosenu_prepare_graphs",
+    "cosenu_synchronize",
     "cosenu_time", "cosenu_analyse", "cosenu_pee_v", "cosenu_init_seeded",
     "cosenu_init_reference", "cosenu_device_state", "cosenu_upload_device",
     "cosenu_download_device", "cosenu_launches_per_step", "cosenu_tile", "cosenu_device_bytes",
@@ -96,6 +97,7 @@ def load(path: str | None = None) -> C.CDLL:
         "cosenu_mark_state0": (i, [vp]),
         "cosenu_step": (i, [vp, i]),
         "cosenu_step_stage": (i, [vp, i]),
+        "cosenu_prepare_graphs": (i, [vp]),
         "cosenu_synchronize": (i, [vp]),
         "cosenu_set_wait_limit": (i, [vp, d]),
         "cosenu_test_stall_pipeline": (i, [vp, i]),

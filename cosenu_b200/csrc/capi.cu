@@ -820,6 +820,26 @@ int cosenu_step(cosenu_ctx *ctx, int nsteps)
     return COSENU_OK;
 }
 
+int cosenu_prepare_graphs(cosenu_ctx *ctx)
+{
+    if (!ctx) return COSENU_ERR_ARG;
+    if (ctx->next_stage != 0) return fail(ctx, COSENU_ERR_STATE, "RK4 step in progress");
+    if (!ctx->use_graphs) return COSENU_OK;
+    DeviceGuard dg(ctx->p.device);
+    // FP32-bulk: graphs for both parities of the state buffer; the context's
+    // parity is put back whatever happens
+    const int npar = ctx->fp32 ? 2 : 1, par0 = ctx->ypar;
+    cudaError_t e = cudaSuccess;
+    for (int i = 0; i < npar && e == cudaSuccess; ++i) {
+        if (i) flip(ctx);
+        if (!ctx->gN[ctx->ypar]) e = capture(ctx, GRAPH_CHUNK, &ctx->gN[ctx->ypar]);
+        if (e == cudaSuccess && !ctx->g1[ctx->ypar]) e = capture(ctx, 1, &ctx->g1[ctx->ypar]);
+    }
+    if (ctx->ypar != par0) flip(ctx);
+    CK(e);
+    return COSENU_OK;
+}
+
 int cosenu_synchronize(cosenu_ctx *ctx)
 {
     if (!ctx) return COSENU_ERR_ARG;

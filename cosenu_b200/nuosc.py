@@ -184,6 +184,10 @@ class NuOsc:
     def step_stage(self, stage: int) -> None:
         self._check(self.lib.cosenu_step_stage(self.h, stage))
 
+    def prepare_graphs(self) -> None:
+        """Capture the CUDA graphs of evolve() now rather than on first use."""
+        self._check(self.lib.cosenu_prepare_graphs(self.h))
+
     def synchronize(self) -> None:
         self._check(self.lib.cosenu_synchronize(self.h))
 

@@ -142,6 +142,12 @@ int cosenu_step(cosenu_ctx *ctx, int nsteps);
  * exposed so that a caller can time the stages separately. */
 int cosenu_step_stage(cosenu_ctx *ctx, int stage);
 
+/* Captures the CUDA graphs cosenu_step launches (a chunk of 16 steps and a
+ * single step, for each state-buffer parity the precision uses) now rather
+ * than on first use, so that no later call pays for a capture.  Launches
+ * nothing; a no-op where graphs are off (COSENU_NO_GRAPH=1). */
+int cosenu_prepare_graphs(cosenu_ctx *ctx);
+
 /* Waits for the context's stream.  COSENU_ERR_CUDA when a pipeline wait of a
  * stage kernel ran out of time (its results are not to be trusted); that
  * report repeats on every later check until a new state is uploaded or

@@ -128,6 +128,31 @@ def test_deterministic_and_graph_equals_stagewise(gpu_lib, oracle):
     assert np.array_equal(outs[0], outs[2])
 
 
+@pytest.mark.parametrize("precision", ["fp64", "fp32"])
+@pytest.mark.parametrize("kernel", ["auto", "tma"])
+def test_prepared_graphs_equal_lazy_capture(gpu_lib, oracle, monkeypatch, precision, kernel):
+    """cosenu_prepare_graphs captures the graphs of both state-buffer parities
+    ahead of use (idempotent, also with the parity flipped by an odd step
+    count); stepping through them equals the lazily captured ones."""
+    if kernel == "tma":
+        monkeypatch.setenv("COSENU_KERNEL", "tma")
+    case, d = load_golden("fv_vac")
+    st0, _, _ = _inputs(case, d, oracle)
+    outs = []
+    for prep in (False, True):
+        with gpu_from_case(case, precision=precision) as sim:
+            sim.upload(st0)
+            if prep:
+                sim.prepare_graphs()
+                sim.prepare_graphs()
+            sim.evolve(3)
+            if prep:
+                sim.prepare_graphs()
+            sim.evolve(37)
+            outs.append(sim.download())
+    assert np.array_equal(outs[0], outs[1])
+
+
 def test_snapshot_is_the_state_at_the_call(gpu_lib, oracle):
     """cosenu_snapshot: the host copy holds the state at the call even when
     more steps are queued before cosenu_snapshot_wait; consecutive snapshots

@@ -190,6 +190,14 @@ template <int SCHEME, class TIN, class TOUT, int STAGE> struct Layout {
     // other kernels keep them in registers and pair warps at the tile's end
     static constexpr bool MSM = SCHEME == FV && (INC || STAGE != 3);
     static constexpr int NRED = MSM ? R : R / 2;  // moment slots in shared memory
+    // FV: the face of each row and component at the tile's upwind edge lies
+    // outside the warp's 32 lanes.  Each chunk, NE = R * NCOMP / 32 warps (in
+    // turn) compute all of them at full lane occupancy and publish them in
+    // shared memory (one slot array and one mbarrier per ring buffer), rather
+    // than every warp spending a ninth WENO7 pass with 8 of 32 lanes active.
+    static constexpr int NE = SCHEME == FV ? R * NCOMP / 32 : 0;
+    static_assert(NE == 0 || (R * NCOMP % 32 == 0 && (R & (R - 1)) == 0),
+                  "edge warps: whole warps, rows a power of two");
 };
 
 // Index of each operand's tensor map among a member's NMAP maps (ensembles).
@@ -261,9 +269,13 @@ __global__ void __launch_bounds__(tma::Layout<SCHEME, TIN, TOUT, STAGE>::NTHR, M
     extern __shared__ __align__(1024) unsigned char smem[];
     uint64_t *full = reinterpret_cast<uint64_t *>(smem + NBUF * L::BUF);
     uint64_t *empty = full + NBUF;
-    double(*s_mom)[TZ] = reinterpret_cast<double(*)[TZ]>(empty + NBUF);  // [6][TZ]
+    uint64_t *ebar = empty + NBUF;  // FV: edge faces of buffer b published
+    double(*s_mom)[TZ] =
+        reinterpret_cast<double(*)[TZ]>(ebar + (L::NE ? NBUF : 0));  // [6][TZ]
     double(*s_red)[NMOM][TZ] = reinterpret_cast<double(*)[NMOM][TZ]>(s_mom + NMOM);  // [NRED]
     StageArgs *s_args = reinterpret_cast<StageArgs *>(s_red + L::NRED);  // batched: current member
+    // FV: [NBUF][R][NCOMP] edge faces
+    double(*s_edge)[R][NCOMP] = reinterpret_cast<double(*)[R][NCOMP]>(s_args + 1);
 
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const int nzt = BATCHED ? bd.ntiles : a0.nz / TZ;
@@ -272,6 +284,7 @@ __global__ void __launch_bounds__(tma::Layout<SCHEME, TIN, TOUT, STAGE>::NTHR, M
         for (int b = 0; b < NBUF; ++b) {
             tma::mbar_init(&full[b], 1);
             tma::mbar_init(&empty[b], R);
+            if (L::NE) tma::mbar_init(&ebar[b], L::NE * 32);
         }
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
@@ -410,63 +423,94 @@ __global__ void __launch_bounds__(tma::Layout<SCHEME, TIN, TOUT, STAGE>::NTHR, M
             const double factor = fac;
             const bool landed = tma::mbar_wait(&full[b], (it / NBUF) & 1, err, 2, a0.wait_ns);
             const unsigned char *buf = smem + b * L::BUF;
-            // this warp's row of component 0 in the input box (HALO cells each
-            // side); the row's components are XW cells apart
+            // row r of component 0 in the input box (HALO cells each side); a
+            // row's components are XW cells apart
             constexpr int XW = L::XW, YW = L::YW;
-            const TIN *xrow = reinterpret_cast<const TIN *>(buf) + warp * (NCOMP * XW) + HALO;
-            const double *yrow = reinterpret_cast<const double *>(buf + L::XB) +
-                                 warp * (NCOMP * YW) + (INC ? HALO : 0);
-            // the stage input at cell j of this row (j in [-HALO, TZ + HALO))
-            auto in = [&](int q, int j) -> double {
-                if constexpr (INC && STAGE >= 2)
-                    return yrow[q * YW + j] + (double)xrow[q * XW + j];
-                else
-                    return (double)xrow[q * XW + j];
+            auto xrow_of = [&](int r) {
+                return reinterpret_cast<const TIN *>(buf) + r * (NCOMP * XW) + HALO;
             };
+            auto yrow_of = [&](int r) {
+                return reinterpret_cast<const double *>(buf + L::XB) + r * (NCOMP * YW) +
+                       (INC ? HALO : 0);
+            };
+            const TIN *xrow = xrow_of(warp);  // this warp's row
+            const double *yrow = yrow_of(warp);
+            // the stage input at cell j of row x / y (j in [-HALO, TZ + HALO))
+            auto in_r = [&](const TIN *x, const double *y, int q, int j) -> double {
+                if constexpr (INC && STAGE >= 2)
+                    return y[q * YW + j] + (double)x[q * XW + j];
+                else
+                    return (double)x[q * XW + j];
+            };
+            auto in = [&](int q, int j) -> double { return in_r(xrow, yrow, q, j); };
             // FP32-bulk: the stencil difference u(j + k) - u(j) as
             // (Y difference in FP64, rounded) + (D difference in FP32)
-            auto dif = [&](int q, int j, int k) -> float {
+            auto dif = [&](const TIN *x, const double *y, int q, int j, int k) -> float {
                 if constexpr (INC && STAGE >= 2)
-                    return (float)(yrow[q * YW + j + k] - yrow[q * YW + j]) +
-                           ((float)xrow[q * XW + j + k] - (float)xrow[q * XW + j]);
+                    return (float)(y[q * YW + j + k] - y[q * YW + j]) +
+                           ((float)x[q * XW + j + k] - (float)x[q * XW + j]);
                 else
-                    return (float)((double)xrow[q * XW + j + k] - (double)xrow[q * XW + j]);
+                    return (float)((double)x[q * XW + j + k] - (double)x[q * XW + j]);
             };
-            // upwind WENO7 face of component q about cell j, stencil direction dir
-            auto face = [&](int q, int j, int dir) -> double {
+            // upwind WENO7 face of component q about cell j of row x / y,
+            // stencil direction dir
+            auto face_r = [&](const TIN *x, const double *y, int q, int j, int dir) -> double {
                 if constexpr (INC) {
-                    const float corr = weno7_corr(dif(q, j, -3 * dir), dif(q, j, -2 * dir),
-                                                  dif(q, j, -dir), dif(q, j, dir),
-                                                  dif(q, j, 2 * dir), dif(q, j, 3 * dir));
+                    const float corr =
+                        weno7_corr(dif(x, y, q, j, -3 * dir), dif(x, y, q, j, -2 * dir),
+                                   dif(x, y, q, j, -dir), dif(x, y, q, j, dir),
+                                   dif(x, y, q, j, 2 * dir), dif(x, y, q, j, 3 * dir));
                     if constexpr (STAGE >= 2)  // Y + (D + correction)
-                        return yrow[q * YW + j] + (double)((float)xrow[q * XW + j] + corr);
+                        return y[q * YW + j] + (double)((float)x[q * XW + j] + corr);
                     else
-                        return (double)xrow[q * XW + j] + (double)corr;
+                        return (double)x[q * XW + j] + (double)corr;
                 } else {
-                    return weno7_face(in(q, j - 3 * dir), in(q, j - 2 * dir), in(q, j - dir),
-                                      in(q, j), in(q, j + dir), in(q, j + 2 * dir),
-                                      in(q, j + 3 * dir));
+                    return weno7_face(in_r(x, y, q, j - 3 * dir), in_r(x, y, q, j - 2 * dir),
+                                      in_r(x, y, q, j - dir), in_r(x, y, q, j),
+                                      in_r(x, y, q, j + dir), in_r(x, y, q, j + 2 * dir),
+                                      in_r(x, y, q, j + 3 * dir));
                 }
             };
+
+            if constexpr (L::NE > 0) {
+                // edge faces of this chunk: warps 2ch, 2ch + 1 (mod R) in turn,
+                // lane -> (row 4h + lane / 8, component lane % 8).  Every lane
+                // arrives, also without advection, so the barrier's phases
+                // follow the ring.
+                const int h = (warp - L::NE * ch) & (R - 1);
+                if (h < L::NE) {
+                    const int r = h * (32 / NCOMP) + (lane >> 3), q = lane & (NCOMP - 1);
+                    if (advec) {
+                        double v2, f2;
+                        row_values<SCHEME>(a.v0, a.dv, a.dz, a.fd_advec,
+                                           min(ch * R + r, a.nvz - 1), v2, f2);
+                        const int d2 = (v2 >= 0.0) ? 1 : -1;
+                        s_edge[b][r][q] = face_r(xrow_of(r), yrow_of(r), q, d2 > 0 ? -1 : TZ, d2);
+                    }
+                    tma::mbar_arrive(&ebar[b]);
+                }
+            }
 
             double c[NCOMP], o[NCOMP], ko[NCOMP];
 #pragma unroll
             for (int q = 0; q < NCOMP; ++q) c[q] = in(q, lane);
             if (SCHEME == FV) {
                 // upwind flux difference (rhs_fv.hpp:143-162): this lane's face
-                // and its neighbour's; lanes 0-7 first build the row's edge faces
+                // and its neighbour's; the face at the tile's upwind edge comes
+                // from the chunk's edge warps (o[] holds the own faces meanwhile)
                 const int dir = (vzv >= 0.0) ? 1 : -1;
-                double edge = 0.0;
-                if (advec && lane < NCOMP) edge = face(lane, dir > 0 ? -1 : TZ, dir);
                 const int src = min(max(lane - dir, 0), TZ - 1);
+#pragma unroll
+                for (int q = 0; q < NCOMP; ++q) o[q] = advec ? face_r(xrow, yrow, q, lane, dir) : 0.0;
+                if (advec) tma::mbar_wait(&ebar[b], (it / NBUF) & 1, err, 2, a0.wait_ns);
 #pragma unroll
                 for (int q = 0; q < NCOMP; ++q) {
                     double adv = 0.0;
                     if (advec) {
-                        const double fown = face(q, lane, dir);
+                        const double fown = o[q];
                         double fnb = __shfl_sync(0xffffffffu, fown, src);
-                        const double e = __shfl_sync(0xffffffffu, edge, q);
-                        if ((dir > 0 && lane == 0) || (dir < 0 && lane == TZ - 1)) fnb = e;
+                        if ((dir > 0 && lane == 0) || (dir < 0 && lane == TZ - 1))
+                            fnb = s_edge[b][warp][q];
                         if (open_bc) {
                             // flux ghosts under OPEN_BC (updateBufferZone on rflux/lflux,
                             // rhs_fv.hpp:118-119): rflux[-1] = rflux[0],
@@ -779,7 +823,8 @@ template <int SCHEME, class TIN, class TOUT, int STAGE>
 static int tma_smem(int NB)
 {
     using L = tma::Layout<SCHEME, TIN, TOUT, STAGE>;
-    return NB * L::BUF + 2 * NB * 8 + (1 + L::NRED) * NMOM * tma::TZ * 8 +
+    return NB * L::BUF + (2 + (L::NE ? 1 : 0)) * NB * 8 + (1 + L::NRED) * NMOM * tma::TZ * 8 +
+           (L::NE ? NB * L::R * NCOMP * 8 : 0) +
            (int)sizeof(StageArgs);
 }
 

@@ -13,8 +13,10 @@
 // flight (~100 KB per SM) the kernel keeps HBM busy without depending on
 // occupancy, which the register-heavy FP64 right-hand side limits.  FD runs
 // one block per SM; FV, bound by FP64 issue rather than HBM, runs two (each
-// with half the shared memory and <= 112 registers per thread) so that twice
-// the warps hide the latency of the WENO7 arithmetic.  Per-row velocities and
+// with half the shared memory) so that twice the warps hide the latency of the
+// WENO7 arithmetic.  A single FV simulation has no producer warp: the last
+// consumer warp to release a buffer issues its next copies, so a block is 8
+// warps and gets 128 registers per thread.  Per-row velocities and
 // advection factors are recomputed in registers, bit-equal to the host tables.
 //
 // FV: a warp holds one row, so every lane reconstructs the upwind WENO7 face it
@@ -28,9 +30,11 @@
 // expiry the kernel records a code in *err and carries on along the same
 // control path, so no barrier is left waiting and the host reports the error.
 // After a failed wait a consumer warp does not release its buffer, so the
-// producer's next wait on that buffer fails too and it stops issuing copies;
-// before it exits it waits (bounded again) for the copies it has in flight, so
-// no block ends while a bulk copy still writes into its shared memory.
+// producer's next wait on that buffer fails too and it stops issuing copies
+// (without a producer warp the buffer's release count never completes and no
+// warp refills it); before the block exits one thread waits (bounded again)
+// for the copies in flight, so no block ends while a bulk copy still writes
+// into its shared memory.
 #include <cuda.h>
 
 #include <type_traits>
@@ -50,8 +54,7 @@ constexpr int HALO = 4;          // cells each side in the input box
 // the same cell of all 8 components at once (42 doubles = 84 words: banks
 // 0, 20, 8, 28, ... for components 0..7; 44 floats = 44 words: 0, 12, 24, ...).
 template <class T> constexpr int xw() { return sizeof(T) == 8 ? 42 : 44; }
-// v rows per chunk = consumer warps.  FV runs two blocks per SM (<= 96
-// registers per thread) with 8.  FD runs one block per SM: the stages that move
+// v rows per chunk = consumer warps.  FV runs two blocks per SM with 8.  FD runs one block per SM: the stages that move
 // few bytes per cell (FP64 stage 1, FP32-bulk stages 1-3) are bound by latency
 // and run 12 (13 warps, ~126 registers, no spills: 0.230 -> 0.205 ms for FP64
 // stage 1 at nz 32768 x nvz 256); the HBM-bound stages keep 8, whose smaller
@@ -170,6 +173,8 @@ template <int SCHEME, class TIN, class TOUT, int STAGE> struct Layout {
     static constexpr bool INC = inc_form<TIN, TOUT>();
     static constexpr int R = rows<SCHEME, STAGE, INC>();
     static constexpr int NTHR = R * 32 + 32;  // consumer warps + producer warp
+    // without a producer warp (see producer_warp)
+    static constexpr int NTHR_NP = R * 32;
     // FP64 stage 3 streams the most bytes per chunk: its 40-cell rows keep a
     // two-buffer ring within half an SM's shared memory (two blocks per SM)
     static constexpr int XW = (!INC && STAGE == 3) ? TZ + 2 * HALO : xw<TIN>();
@@ -184,7 +189,7 @@ template <int SCHEME, class TIN, class TOUT, int STAGE> struct Layout {
     static constexpr int AB = INC ? (STAGE == 4 ? 2 * NCOMP * R * TZ * 4 : 0)
                                   : (STAGE >= 3 ? NCOMP * R * TZ * 8 : 0);
     static constexpr int BUF = ((XB + YB + AB) + 127) / 128 * 128;
-    // FV (two blocks per SM, <= 96 registers): each consumer warp accumulates
+    // FV (two blocks per SM, 96-128 registers): each consumer warp accumulates
     // the output moments of its rows in shared memory rather than in 12
     // registers, where half an SM leaves room (all but FP64 stage 3); the
     // other kernels keep them in registers and pair warps at the tile's end
@@ -199,6 +204,53 @@ template <int SCHEME, class TIN, class TOUT, int STAGE> struct Layout {
     static_assert(NE == 0 || (R * NCOMP % 32 == 0 && (R & (R - 1)) == 0),
                   "edge warps: whole warps, rows a power of two");
 };
+
+// FD and ensemble launches stream through a producer warp.  A single FV
+// simulation runs without one: the last consumer warp to release a ring
+// buffer issues that buffer's next copies itself.  Its block is then 8 warps,
+// and two blocks per SM get 128 registers per thread instead of the 96 that
+// two 9-warp blocks leave (FP64 stage 3 spilled at 96).
+template <int SCHEME, bool BATCHED> __host__ __device__ constexpr bool producer_warp()
+{
+    return SCHEME == FD || BATCHED;
+}
+
+// Arrival counter of a ring buffer without a producer warp: acquire-release
+// add, so the last warp's refill is ordered after every warp's reads.
+__device__ __forceinline__ uint32_t ring_release_count(uint32_t *cnt)
+{
+    uint32_t old;
+    asm volatile("atom.acq_rel.cta.shared::cta.add.u32 %0, [%1], 1;"
+                 : "=r"(old)
+                 : "r"(smem_u32(cnt))
+                 : "memory");
+    return old;
+}
+
+// Orders this thread's generic-proxy view of shared memory before the bulk
+// copies it issues next.
+__device__ __forceinline__ void fence_proxy_async_smem()
+{
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+
+// The copies of one ring buffer: the stage input box (X) and, where the
+// stage reads them, Y and the own-cell tiles A (and B), all completing on
+// `bar`.  Coordinates: (cell, component 0, first row of the chunk).
+template <class L>
+__device__ __forceinline__ void issue_chunk(unsigned char *buf, uint64_t *bar, const CUtensorMap *px,
+                                            const CUtensorMap *py, const CUtensorMap *pa,
+                                            const CUtensorMap *pb, int z0, int row0)
+{
+    mbar_expect_tx(bar, L::XB + L::YB + L::AB);
+    tma_load_3d(buf, px, HP + z0 - HALO, 0, row0, bar);
+    if (L::YB) tma_load_3d(buf + L::XB, py, HP + z0 - (L::INC ? HALO : 0), 0, row0, bar);
+    if (L::AB && !L::INC) tma_load_3d(buf + L::XB + L::YB, pa, HP + z0, 0, row0, bar);
+    if (L::AB && L::INC) {
+        tma_load_3d(buf + L::XB + L::YB, pa, HP + z0, 0, row0, bar);
+        tma_load_3d(buf + L::XB + L::YB + L::AB / 2, pb, HP + z0, 0, row0, bar);
+    }
+}
 
 // Index of each operand's tensor map among a member's NMAP maps (ensembles).
 // FP64:      0 Y (halo box), 1 U0 (halo), 2 U1 (halo), 3 Y (tile), 4 A (tile), 5 U0 (tile)
@@ -253,7 +305,10 @@ __device__ __forceinline__ void row_values(double v0, double dv, double dz, int 
 // right-hand side is evaluated in FP64 in both forms, except the FP32-bulk
 // WENO7 weights and candidates (FP32 on FP64 stencil differences).
 template <int SCHEME, bool GEN, int STAGE, class TIN, class TOUT, int NBUF, bool BATCHED, int MINB>
-__global__ void __launch_bounds__(tma::Layout<SCHEME, TIN, TOUT, STAGE>::NTHR, MINB)
+__global__ void __launch_bounds__(tma::producer_warp<SCHEME, BATCHED>()
+                                      ? tma::Layout<SCHEME, TIN, TOUT, STAGE>::NTHR
+                                      : tma::Layout<SCHEME, TIN, TOUT, STAGE>::NTHR_NP,
+                                  MINB)
     rk4_stage_tma_kernel(const __grid_constant__ CUtensorMap mX,
                          const __grid_constant__ CUtensorMap mY,
                          const __grid_constant__ CUtensorMap mA,
@@ -276,21 +331,44 @@ __global__ void __launch_bounds__(tma::Layout<SCHEME, TIN, TOUT, STAGE>::NTHR, M
     StageArgs *s_args = reinterpret_cast<StageArgs *>(s_red + L::NRED);  // batched: current member
     // FV: [NBUF][R][NCOMP] edge faces
     double(*s_edge)[R][NCOMP] = reinterpret_cast<double(*)[R][NCOMP]>(s_args + 1);
+    // without a producer warp: per ring buffer, the warps' release count and
+    // the last chunk whose copies went into it
+    constexpr bool PW = producer_warp<SCHEME, BATCHED>();
+    uint32_t *s_cnt = reinterpret_cast<uint32_t *>(s_edge + (L::NE ? NBUF : 0));
+    int *s_last = reinterpret_cast<int *>(s_cnt + NBUF);
 
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const int nzt = BATCHED ? bd.ntiles : a0.nz / TZ;
+    // without a producer warp (single simulation): chunk n of this block is
+    // chunk n % nch1 of its (n / nch1)-th z tile; its copies go into buffer
+    // n % NBUF
+    const int nch1 = (a0.nvz + R - 1) / R;
+    auto refill = [&](uint32_t n) {
+        const int t = blockIdx.x + (int)(n / nch1) * gridDim.x;
+        if (t >= nzt || a0.stall) return;
+        const int b = n % NBUF;
+        issue_chunk<L>(smem + b * L::BUF, &full[b], &mX, &mY, &mA, &mB, t * TZ,
+                       (int)(n % nch1) * R);
+        s_last[b] = (int)n;
+    };
 
     if (tid == 0) {
         for (int b = 0; b < NBUF; ++b) {
             tma::mbar_init(&full[b], 1);
             tma::mbar_init(&empty[b], R);
             if (L::NE) tma::mbar_init(&ebar[b], L::NE * 32);
+            if constexpr (!PW) {
+                s_cnt[b] = 0;
+                s_last[b] = -1;
+            }
         }
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        if constexpr (!PW)
+            for (int b = 0; b < NBUF; ++b) refill(b);
     }
     __syncthreads();
 
-    if (warp == R) {
+    if (PW && warp == R) {
         // ------------------------------------------------------------ producer
         if (lane == 0 && !a0.stall) {
             uint32_t it = 0;
@@ -329,20 +407,7 @@ __global__ void __launch_bounds__(tma::Layout<SCHEME, TIN, TOUT, STAGE>::NTHR, M
                         issuing = false;  // a consumer gave up: buffer b may still be in use
                         break;
                     }
-                    unsigned char *buf = smem + b * L::BUF;
-                    tma::mbar_expect_tx(&full[b], L::XB + L::YB + L::AB);
-                    // coordinates: (cell, component 0, first row of the chunk)
-                    tma::tma_load_3d(buf, px, HP + z0 - HALO, 0, ch * R, &full[b]);
-                    if (L::YB)
-                        tma::tma_load_3d(buf + L::XB, py, HP + z0 - (INC ? HALO : 0), 0, ch * R,
-                                         &full[b]);
-                    if (L::AB && !INC)
-                        tma::tma_load_3d(buf + L::XB + L::YB, pa, HP + z0, 0, ch * R, &full[b]);
-                    if (L::AB && INC) {
-                        tma::tma_load_3d(buf + L::XB + L::YB, pa, HP + z0, 0, ch * R, &full[b]);
-                        tma::tma_load_3d(buf + L::XB + L::YB + L::AB / 2, pb, HP + z0, 0, ch * R,
-                                         &full[b]);
-                    }
+                    issue_chunk<L>(smem + b * L::BUF, &full[b], px, py, pa, pb, z0, ch * R);
                 }
                 cur = nxt;
             }
@@ -669,9 +734,19 @@ __global__ void __launch_bounds__(tma::Layout<SCHEME, TIN, TOUT, STAGE>::NTHR, M
                 }
             }
             // this warp is done with the buffer (after a failed wait it keeps
-            // the buffer: the producer's wait on it fails and it stops issuing)
+            // the buffer: the producer's wait on it fails and it stops issuing;
+            // without a producer, the count never completes and no warp
+            // refills the buffer)
             __syncwarp();
-            if (lane == 0 && landed) tma::mbar_arrive(&empty[b]);
+            if (lane == 0 && landed) {
+                if constexpr (PW) {
+                    tma::mbar_arrive(&empty[b]);
+                } else if (ring_release_count(&s_cnt[b]) == (it / NBUF) * R + (R - 1)) {
+                    // the last of the R warps to release buffer b: its next chunk
+                    fence_proxy_async_smem();
+                    refill(it + NBUF);
+                }
+            }
 
             TOUT uleft[NCOMP];
             if (open_bc) {
@@ -764,6 +839,15 @@ __global__ void __launch_bounds__(tma::Layout<SCHEME, TIN, TOUT, STAGE>::NTHR, M
         }
         cur = nxt;
     }
+    if constexpr (!PW) {
+        // the last copies issued into each buffer have landed before the block
+        // exits (in normal operation the consumers have waited for them)
+        consumer_sync();
+        if (tid == 0)
+            for (int b = 0; b < NBUF; ++b)
+                if (s_last[b] >= 0)
+                    tma::mbar_drain(&full[b], ((uint32_t)s_last[b] / NBUF) & 1, err, a0.wait_ns);
+    }
 }
 
 // ---------------------------------------------------------------------------
@@ -825,7 +909,7 @@ static int tma_smem(int NB)
     using L = tma::Layout<SCHEME, TIN, TOUT, STAGE>;
     return NB * L::BUF + (2 + (L::NE ? 1 : 0)) * NB * 8 + (1 + L::NRED) * NMOM * tma::TZ * 8 +
            (L::NE ? NB * L::R * NCOMP * 8 : 0) +
-           (int)sizeof(StageArgs);
+           (int)sizeof(StageArgs) + NB * 8;  // + release counts, last chunks
 }
 
 static int tma_smem_limit(int minb)
@@ -857,9 +941,10 @@ static cudaError_t launch_nb(const StageMaps &m, const StageArgs &a, int *err, i
         return cudaSuccess;
     }
     const int shmem = tma_smem<SCHEME, TIN, TOUT, STAGE>(NB);
-    constexpr int NT = tma::Layout<SCHEME, TIN, TOUT, STAGE>::NTHR;
+    using L = tma::Layout<SCHEME, TIN, TOUT, STAGE>;
+    constexpr int NT = tma::producer_warp<SCHEME, false>() ? L::NTHR : L::NTHR_NP;
     if (bd)
-        kernb<<<nblocks, NT, shmem, s>>>(*m.x, *m.y, *m.a, *m.b, a, err, *bd);
+        kernb<<<nblocks, L::NTHR, shmem, s>>>(*m.x, *m.y, *m.a, *m.b, a, err, *bd);
     else
         kern<<<nblocks, NT, shmem, s>>>(*m.x, *m.y, *m.a, *m.b, a, err, BatchDev{});
     return cudaGetLastError();

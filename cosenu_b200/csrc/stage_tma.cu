@@ -536,6 +536,15 @@ __global__ void __launch_bounds__(tma::producer_warp<SCHEME, BATCHED>()
                                       in_r(x, y, q, j + 3 * dir));
                 }
             };
+            // FP64: numerator and denominator of that face (face = centre +
+            // num / den); the faces of components 0-3 and 4-7 of a row then
+            // share one division (recip4)
+            auto parts_r = [&](const TIN *x, const double *y, int q, int j, int dir, double &num,
+                               double &den) {
+                weno7_parts(in_r(x, y, q, j - 3 * dir), in_r(x, y, q, j - 2 * dir),
+                            in_r(x, y, q, j - dir), in_r(x, y, q, j), in_r(x, y, q, j + dir),
+                            in_r(x, y, q, j + 2 * dir), in_r(x, y, q, j + 3 * dir), num, den);
+            };
 
             if constexpr (L::NE > 0) {
                 // edge faces of this chunk: warps 2ch, 2ch + 1 (mod R) in turn,
@@ -550,7 +559,23 @@ __global__ void __launch_bounds__(tma::producer_warp<SCHEME, BATCHED>()
                         row_values<SCHEME>(a.v0, a.dv, a.dz, a.fd_advec,
                                            min(ch * R + r, a.nvz - 1), v2, f2);
                         const int d2 = (v2 >= 0.0) ? 1 : -1;
-                        s_edge[b][r][q] = face_r(xrow_of(r), yrow_of(r), q, d2 > 0 ? -1 : TZ, d2);
+                        const int je = d2 > 0 ? -1 : TZ;
+                        if constexpr (INC) {
+                            s_edge[b][r][q] = face_r(xrow_of(r), yrow_of(r), q, je, d2);
+                        } else {
+                            // the row's four denominators of this component group
+                            // sit in lanes 4k..4k+3: the same division as the
+                            // neighbouring tile's own face, bit for bit
+                            double num, den, i[4];
+                            parts_r(xrow_of(r), yrow_of(r), q, je, d2, num, den);
+                            recip4(__shfl_sync(0xffffffffu, den, 0, 4),
+                                   __shfl_sync(0xffffffffu, den, 1, 4),
+                                   __shfl_sync(0xffffffffu, den, 2, 4),
+                                   __shfl_sync(0xffffffffu, den, 3, 4), i[0], i[1], i[2], i[3]);
+                            const int k = q & 3;
+                            const double inv = k == 0 ? i[0] : k == 1 ? i[1] : k == 2 ? i[2] : i[3];
+                            s_edge[b][r][q] = __fma_rn(num, inv, in_r(xrow_of(r), yrow_of(r), q, je));
+                        }
                     }
                     tma::mbar_arrive(&ebar[b]);
                 }
@@ -565,8 +590,27 @@ __global__ void __launch_bounds__(tma::producer_warp<SCHEME, BATCHED>()
                 // from the chunk's edge warps (o[] holds the own faces meanwhile)
                 const int dir = (vzv >= 0.0) ? 1 : -1;
                 const int src = min(max(lane - dir, 0), TZ - 1);
+                if constexpr (INC) {
 #pragma unroll
-                for (int q = 0; q < NCOMP; ++q) o[q] = advec ? face_r(xrow, yrow, q, lane, dir) : 0.0;
+                    for (int q = 0; q < NCOMP; ++q)
+                        o[q] = advec ? face_r(xrow, yrow, q, lane, dir) : 0.0;
+                } else {
+                    double den[NCOMP];
+#pragma unroll
+                    for (int q = 0; q < NCOMP; ++q) {
+                        o[q] = 0.0;
+                        den[q] = 1.0;
+                        if (advec) parts_r(xrow, yrow, q, lane, dir, o[q], den[q]);
+                    }
+#pragma unroll
+                    for (int g = 0; g < NCOMP; g += 4) {
+                        double i[4];
+                        recip4(den[g], den[g + 1], den[g + 2], den[g + 3], i[0], i[1], i[2], i[3]);
+#pragma unroll
+                        for (int k = 0; k < 4; ++k)
+                            o[g + k] = advec ? __fma_rn(o[g + k], i[k], c[g + k]) : 0.0;
+                    }
+                }
                 if (advec) tma::mbar_wait(&ebar[b], (it / NBUF) & 1, err, 2, a0.wait_ns);
 #pragma unroll
                 for (int q = 0; q < NCOMP; ++q) {

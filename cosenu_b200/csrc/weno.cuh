@@ -14,10 +14,11 @@ namespace cosenu {
 // from the centre value d (the indicators are invariant under a constant
 // shift and each candidate's weights sum to 12, so the face is d plus the
 // weighted differences: 15 fewer FP64 operations per face and less
-// cancellation), and the four weights are brought to a common denominator so
-// that the face needs one division.
-__device__ __forceinline__ double weno7_face(double a, double b, double c, double d, double e,
-                                             double f, double g)
+// cancellation), and the four weights are brought to a common denominator,
+// so that the face is d + num / den.  gamma (and the 12) ride on the
+// candidates' integer coefficients and on den, not on the weights.
+__device__ __forceinline__ void weno7_parts(double a, double b, double c, double d, double e,
+                                            double f, double g, double &num, double &den)
 {
     const double eps = 1e-6;
     const double A = a - d, B = b - d, Cc = c - d, E = e - d, F = f - d, G = g - d;
@@ -29,23 +30,47 @@ __device__ __forceinline__ double weno7_face(double a, double b, double c, doubl
                 547. * E * E;
     double s3 = A * (547. * A - 3882. * B + 4642. * Cc) + B * (7043. * B - 17246. * Cc) +
                 11003. * Cc * Cc;
-    // 12 x (candidate value - d): each candidate's weights sum to 12
-    double q0 = 13. * E - 5. * F + G;
-    double q1 = -Cc + 7. * E - F;
-    double q2 = B - 5. * Cc + 3. * E;
+    // gamma_r x 12 x (candidate value - d): each candidate's weights sum to 12
+    double q0 = 52. * E - 20. * F + 4. * G;
+    double q1 = -18. * Cc + 126. * E - 18. * F;
+    double q2 = 12. * B - 60. * Cc + 36. * E;
     double q3 = -3. * A + 13. * B - 23. * Cc;
     double d0 = (eps + s0) * (eps + s0);
     double d1 = (eps + s1) * (eps + s1);
     double d2 = (eps + s2) * (eps + s2);
     double d3 = (eps + s3) * (eps + s3);
     double d01 = d0 * d1, d23 = d2 * d3;
-    double w0 = 4. * d1 * d23;
-    double w1 = 18. * d0 * d23;
-    double w2 = 12. * d01 * d3;
-    double w3 = d01 * d2;
-    double num = w0 * q0 + w1 * q1 + w2 * q2 + w3 * q3;
-    double den = 12. * (w0 + w1 + w2 + w3);
+    // the weights without gamma: w_r = prod_{k != r} d_k
+    double w0 = d1 * d23, w1 = d0 * d23, w2 = d01 * d3, w3 = d01 * d2;
+    num = w0 * q0 + w1 * q1 + w2 * q2 + w3 * q3;
+    den = 48. * w0 + 216. * w1 + 144. * w2 + 12. * w3;
+}
+
+__device__ __forceinline__ double weno7_face(double a, double b, double c, double d, double e,
+                                             double f, double g)
+{
+    double num, den;
+    weno7_parts(a, b, c, d, e, f, g, num, den);
     return d + num / den;
+}
+
+// 1 / D0 .. 1 / D3 from one division: the product of the four, its
+// reciprocal, then products of the others.  Denominators of weno7_parts lie
+// in [4e-34, 2e34] where the stencil differences are at most 2 in magnitude
+// (density-matrix entries of O(1)), so the product of four stays far inside
+// the FP64 range.  Explicit round-to-nearest operations: the same
+// inputs give the same bits wherever this is evaluated (the face of a tile's
+// edge row is computed by two different warps).
+__device__ __forceinline__ void recip4(double D0, double D1, double D2, double D3, double &i0,
+                                       double &i1, double &i2, double &i3)
+{
+    const double p01 = __dmul_rn(D0, D1), p23 = __dmul_rn(D2, D3);
+    const double r = 1.0 / __dmul_rn(p01, p23);
+    const double r01 = __dmul_rn(r, p23), r23 = __dmul_rn(r, p01);
+    i0 = __dmul_rn(r01, D1);
+    i1 = __dmul_rn(r01, D0);
+    i2 = __dmul_rn(r23, D3);
+    i3 = __dmul_rn(r23, D2);
 }
 
 // FP32-bulk form: the face value minus the centre value from the six

@@ -144,6 +144,9 @@ StageArgs stage_args(const cosenu_ctx *ctx, int stage, int par)
     a.ct = ctx->ct;
     a.st = ctx->st;
     a.pmo = ctx->p.pmo;
+    // omega = 0 (or no mass-ordering sign): the vacuum terms are exact zeros,
+    // and the stage kernels skip them
+    if ((a.ct == 0.0 && a.st == 0.0) || a.pmo == 0.0) a.flags &= ~F_VAC;
     const double ko = 1.0e-1;  // src/nuosc.hpp:60
     a.ko_eps = ctx->p.ko_order == 5 ? -ko / ctx->dz / 64.0 : -ko / ctx->dz / 16.0;
     a.wait_ns = ctx->wait_ns;

@@ -17,7 +17,9 @@
 // WENO7 arithmetic.  A single FV simulation has no producer warp: the last
 // consumer warp to release a buffer issues its next copies, so a block is 8
 // warps and gets 128 registers per thread.  Per-row velocities and
-// advection factors are recomputed in registers, bit-equal to the host tables.
+// advection factors equal the host's tables (src/nuosc.hpp:88-92,
+// rhs_fv.hpp:145, rhs_fd.hpp:57): FV reads them once per chunk through the
+// read-only cache, FD recomputes them in registers.
 //
 // FV: a warp holds one row, so every lane reconstructs the upwind WENO7 face it
 // owns from the shared-memory stencil and takes its neighbour's face by
@@ -280,23 +282,20 @@ __device__ __forceinline__ void tma_tile(const BatchDev &bd, int t, int &inst, i
     }
 }
 
-// Velocity and advection factor of row i, recomputed with round-to-nearest
+// FD: velocity and advection factor of row i, recomputed with round-to-nearest
 // operations so the bits equal the host tables (capi.cu, src/nuosc.hpp:88-92,
-// rhs_fv.hpp:145, rhs_fd.hpp:57): no per-row table occupies shared memory.
-template <int SCHEME>
-__device__ __forceinline__ void row_values(double v0, double dv, double dz, int fd_advec, int i,
-                                           double &v, double &f)
+// rhs_fd.hpp:57).  The FD stages are bound by memory latency, and a table load
+// per chunk slowed them (FP64 stages 1, 2, 4 at nz 32768 x nvz 256 by 8 %); the
+// FP64-bound FV stages read the tables instead.
+__device__ __forceinline__ void fd_row_values(double v0, double dv, double dz, int fd_advec, int i,
+                                              double &v, double &f)
 {
     v = __dadd_rn(v0, __dmul_rn(__dadd_rn((double)i, 0.5), dv));
-    if (SCHEME == FV) {
-        f = __ddiv_rn(-v, dz);
-    } else {
-        const double sv = (double)((0.0 < v) - (v < 0.0));
-        const double d12 = __dmul_rn(12.0, dz);
-        if (fd_advec == 0) f = __ddiv_rn(-v, d12);          // centre
-        else if (fd_advec == 1) f = __ddiv_rn(__dmul_rn(-sv, v), d12);  // upwind
-        else f = __ddiv_rn(__dmul_rn(sv, v), d12);                       // lopsided
-    }
+    const double sv = (double)((0.0 < v) - (v < 0.0));
+    const double d12 = __dmul_rn(12.0, dz);
+    if (fd_advec == 0) f = __ddiv_rn(-v, d12);                      // centre
+    else if (fd_advec == 1) f = __ddiv_rn(__dmul_rn(-sv, v), d12);  // upwind
+    else f = __ddiv_rn(__dmul_rn(sv, v), d12);                       // lopsided
 }
 
 // TIN: type of the streamed stage input (FP64: the stage value U or Y;
@@ -483,9 +482,15 @@ __global__ void __launch_bounds__(tma::producer_warp<SCHEME, BATCHED>()
             const int v = ch * R + warp;
             const bool valid = v < a.nvz;
             const int vr = valid ? v : a.nvz - 1;
-            double vzv, fac;
-            row_values<SCHEME>(a.v0, a.dv, a.dz, a.fd_advec, vr, vzv, fac);
-            const double factor = fac;
+            // the row's velocity and advection factor: FV from the host tables
+            // (read before the wait, so the load overlaps it), FD recomputed
+            double vzv, factor;
+            if constexpr (SCHEME == FV) {
+                vzv = __ldg(&a.vz[vr]);
+                factor = __ldg(&a.rowfac[vr]);
+            } else {
+                fd_row_values(a.v0, a.dv, a.dz, a.fd_advec, vr, vzv, factor);
+            }
             const bool landed = tma::mbar_wait(&full[b], (it / NBUF) & 1, err, 2, a0.wait_ns);
             const unsigned char *buf = smem + b * L::BUF;
             // row r of component 0 in the input box (HALO cells each side); a
@@ -555,9 +560,7 @@ __global__ void __launch_bounds__(tma::producer_warp<SCHEME, BATCHED>()
                 if (h < L::NE) {
                     const int r = h * (32 / NCOMP) + (lane >> 3), q = lane & (NCOMP - 1);
                     if (advec) {
-                        double v2, f2;
-                        row_values<SCHEME>(a.v0, a.dv, a.dz, a.fd_advec,
-                                           min(ch * R + r, a.nvz - 1), v2, f2);
+                        const double v2 = __ldg(&a.vz[min(ch * R + r, a.nvz - 1)]);
                         const int d2 = (v2 >= 0.0) ? 1 : -1;
                         const int je = d2 > 0 ? -1 : TZ;
                         if constexpr (INC) {

@@ -14,9 +14,9 @@
 // occupancy, which the register-heavy FP64 right-hand side limits.  FD runs
 // one block per SM; FV, bound by FP64 issue rather than HBM, runs two (each
 // with half the shared memory) so that twice the warps hide the latency of the
-// WENO7 arithmetic.  A single FV simulation has no producer warp: the last
-// consumer warp to release a buffer issues its next copies, so a block is 8
-// warps and gets 128 registers per thread.  Per-row velocities and
+// WENO7 arithmetic.  FV launches have no producer warp: the last consumer
+// warp to release a buffer issues its next copies, so a block is 8 warps and
+// gets 128 registers per thread.  Per-row velocities and
 // advection factors equal the host's tables (src/nuosc.hpp:88-92,
 // rhs_fv.hpp:145, rhs_fd.hpp:57): FV reads them once per chunk through the
 // read-only cache, FD recomputes them in registers.
@@ -207,14 +207,14 @@ template <int SCHEME, class TIN, class TOUT, int STAGE> struct Layout {
                   "edge warps: whole warps, rows a power of two");
 };
 
-// FD and ensemble launches stream through a producer warp.  A single FV
-// simulation runs without one: the last consumer warp to release a ring
-// buffer issues that buffer's next copies itself.  Its block is then 8 warps,
-// and two blocks per SM get 128 registers per thread instead of the 96 that
-// two 9-warp blocks leave (FP64 stage 3 spilled at 96).
+// FD launches stream through a producer warp.  FV launches (single
+// simulations and ensembles) run without one: the last consumer warp to
+// release a ring buffer issues that buffer's next copies itself.  Its block is
+// then 8 warps, and two blocks per SM get 128 registers per thread instead of
+// the 96 that two 9-warp blocks leave (FP64 stage 3 spilled at 96).
 template <int SCHEME, bool BATCHED> __host__ __device__ constexpr bool producer_warp()
 {
-    return SCHEME == FD || BATCHED;
+    return SCHEME == FD;
 }
 
 // Arrival counter of a ring buffer without a producer warp: acquire-release
@@ -338,17 +338,36 @@ __global__ void __launch_bounds__(tma::producer_warp<SCHEME, BATCHED>()
 
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const int nzt = BATCHED ? bd.ntiles : a0.nz / TZ;
-    // without a producer warp (single simulation): chunk n of this block is
-    // chunk n % nch1 of its (n / nch1)-th z tile; its copies go into buffer
-    // n % NBUF
-    const int nch1 = (a0.nvz + R - 1) / R;
-    auto refill = [&](uint32_t n) {
-        const int t = blockIdx.x + (int)(n / nch1) * gridDim.x;
-        if (t >= nzt || a0.stall) return;
+    // without a producer warp: the block's chunks in order (its z tiles or
+    // table entries, each in chunks of R rows); chunk ch of tile t is the
+    // block's n-th chunk, and its copies go into buffer n % NBUF
+    const bool rr0 = !BATCHED || bd.range == nullptr;
+    const int te0 = rr0 ? nzt : bd.range[blockIdx.x + 1];
+    const int ts0 = rr0 ? gridDim.x : 1;
+    auto nch_of = [&](int t) { return ((BATCHED ? bd.table[t].w : a0.nvz) + R - 1) / R; };
+    auto issue_at = [&](int t, int ch, uint32_t n) {
+        if (a0.stall) return;
         const int b = n % NBUF;
-        issue_chunk<L>(smem + b * L::BUF, &full[b], &mX, &mY, &mA, &mB, t * TZ,
-                       (int)(n % nch1) * R);
+        if constexpr (BATCHED) {
+            const int4 e = bd.table[t];
+            const CUtensorMap *m = &bd.maps[e.x * NMAP];
+            issue_chunk<L>(smem + b * L::BUF, &full[b], &m[MI::X], &m[MI::Y], &m[MI::A],
+                           &m[MI::B], e.y * TZ, ch * R);
+        } else {
+            issue_chunk<L>(smem + b * L::BUF, &full[b], &mX, &mY, &mA, &mB, t * TZ, ch * R);
+        }
         s_last[b] = (int)n;
+    };
+    // (t, ch) moved k chunks on; false past the block's last tile
+    auto advance = [&](int &t, int &ch, int k) -> bool {
+        for (; k > 0; --k) {
+            if (++ch == nch_of(t)) {
+                ch = 0;
+                t += ts0;
+                if (t >= te0) return false;
+            }
+        }
+        return true;
     };
 
     if (tid == 0) {
@@ -362,8 +381,14 @@ __global__ void __launch_bounds__(tma::producer_warp<SCHEME, BATCHED>()
             }
         }
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-        if constexpr (!PW)
-            for (int b = 0; b < NBUF; ++b) refill(b);
+        if constexpr (!PW) {
+            int t = rr0 ? blockIdx.x : bd.range[blockIdx.x], ch = 0;
+            if (t < te0)
+                for (uint32_t n = 0; n < (uint32_t)NBUF; ++n) {
+                    issue_at(t, ch, n);
+                    if (!advance(t, ch, 1)) break;
+                }
+        }
     }
     __syncthreads();
 
@@ -791,7 +816,8 @@ __global__ void __launch_bounds__(tma::producer_warp<SCHEME, BATCHED>()
                 } else if (ring_release_count(&s_cnt[b]) == (it / NBUF) * R + (R - 1)) {
                     // the last of the R warps to release buffer b: its next chunk
                     fence_proxy_async_smem();
-                    refill(it + NBUF);
+                    int t2 = t, ch2 = ch;
+                    if (advance(t2, ch2, NBUF)) issue_at(t2, ch2, it + NBUF);
                 }
             }
 
@@ -991,7 +1017,7 @@ static cudaError_t launch_nb(const StageMaps &m, const StageArgs &a, int *err, i
     using L = tma::Layout<SCHEME, TIN, TOUT, STAGE>;
     constexpr int NT = tma::producer_warp<SCHEME, false>() ? L::NTHR : L::NTHR_NP;
     if (bd)
-        kernb<<<nblocks, L::NTHR, shmem, s>>>(*m.x, *m.y, *m.a, *m.b, a, err, *bd);
+        kernb<<<nblocks, NT, shmem, s>>>(*m.x, *m.y, *m.a, *m.b, a, err, *bd);
     else
         kern<<<nblocks, NT, shmem, s>>>(*m.x, *m.y, *m.a, *m.b, a, err, BatchDev{});
     return cudaGetLastError();

@@ -15,8 +15,9 @@ namespace cosenu {
 // shift and each candidate's weights sum to 12, so the face is d plus the
 // weighted differences: 15 fewer FP64 operations per face and less
 // cancellation), and the four weights are brought to a common denominator,
-// so that the face is d + num / den.  gamma (and the 12) ride on the
-// candidates' integer coefficients and on den, not on the weights.
+// so that the face is d + num / den.  gamma and the 12 ride on the
+// candidates' coefficients (gamma_r / 12 x the integer weights) and gamma on
+// den, not on the weights; den = 4 w0 + 18 w1 + 12 w2 + w3 is three FMAs.
 __device__ __forceinline__ void weno7_parts(double a, double b, double c, double d, double e,
                                             double f, double g, double &num, double &den)
 {
@@ -30,11 +31,12 @@ __device__ __forceinline__ void weno7_parts(double a, double b, double c, double
                 547. * E * E;
     double s3 = A * (547. * A - 3882. * B + 4642. * Cc) + B * (7043. * B - 17246. * Cc) +
                 11003. * Cc * Cc;
-    // gamma_r x 12 x (candidate value - d): each candidate's weights sum to 12
-    double q0 = 52. * E - 20. * F + 4. * G;
-    double q1 = -18. * Cc + 126. * E - 18. * F;
-    double q2 = 12. * B - 60. * Cc + 36. * E;
-    double q3 = -3. * A + 13. * B - 23. * Cc;
+    // gamma_r x (candidate value - d): 12 x (candidate - d) has integer
+    // weights summing to 12, scaled here by gamma_r / 12 = 1/3, 3/2, 1, 1/12
+    double q0 = (13. / 3.) * E - (5. / 3.) * F + (1. / 3.) * G;
+    double q1 = -1.5 * Cc + 10.5 * E - 1.5 * F;
+    double q2 = B - 5. * Cc + 3. * E;
+    double q3 = -0.25 * A + (13. / 12.) * B - (23. / 12.) * Cc;
     double d0 = (eps + s0) * (eps + s0);
     double d1 = (eps + s1) * (eps + s1);
     double d2 = (eps + s2) * (eps + s2);
@@ -43,7 +45,7 @@ __device__ __forceinline__ void weno7_parts(double a, double b, double c, double
     // the weights without gamma: w_r = prod_{k != r} d_k
     double w0 = d1 * d23, w1 = d0 * d23, w2 = d01 * d3, w3 = d01 * d2;
     num = w0 * q0 + w1 * q1 + w2 * q2 + w3 * q3;
-    den = 48. * w0 + 216. * w1 + 144. * w2 + 12. * w3;
+    den = w3 + 4. * w0 + 18. * w1 + 12. * w2;
 }
 
 __device__ __forceinline__ double weno7_face(double a, double b, double c, double d, double e,
@@ -56,7 +58,7 @@ __device__ __forceinline__ double weno7_face(double a, double b, double c, doubl
 
 // 1 / D0 .. 1 / D3 from one division: the product of the four, its
 // reciprocal, then products of the others.  Denominators of weno7_parts lie
-// in [4e-34, 2e34] where the stencil differences are at most 2 in magnitude
+// in [3e-35, 2e33] where the stencil differences are at most 2 in magnitude
 // (density-matrix entries of O(1)), so the product of four stays far inside
 // the FP64 range.  Explicit round-to-nearest operations: the same
 // inputs give the same bits wherever this is evaluated (the face of a tile's

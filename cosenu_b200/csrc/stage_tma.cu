@@ -23,8 +23,9 @@
 //
 // FV: a warp holds one row, so every lane reconstructs the upwind WENO7 face it
 // owns from the shared-memory stencil and takes its neighbour's face by
-// shuffle; the one face per row outside the tile (8 components) is computed by
-// lanes 0-7 in one extra round.  FD: the common variant of manage.py (central
+// shuffle; the one face per row and component outside the tile is computed,
+// for all rows of a chunk at once, by R*8/32 warps in turn and published in
+// shared memory (Layout::NE).  FD: the common variant of manage.py (central
 // FD4 + KO3) is a compile-time fast path; the upwind / lopsided / KO5 variants
 // take the generic path.
 //

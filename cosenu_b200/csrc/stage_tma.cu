@@ -1054,7 +1054,7 @@ static int tma_fd_ring()
 }
 
 // Blocks per SM.  FD (memory bound): one, with the deepest ring that fits.
-// FV (FP64 bound, 9 warps per block): two, to hide FP64 and shared-memory
+// FV (FP64 bound, 8 warps per block): two, to hide FP64 and shared-memory
 // latency with twice the warps, each with the deepest ring that fits in half
 // the SM (COSENU_TMA_MINB=1 selects one block per SM with a 4-deep ring).
 static int tma_minb_env()
